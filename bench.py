@@ -1,0 +1,303 @@
+#!/usr/bin/env python
+"""Benchmark: continuous subgraph matching on one B200 (config 2).
+
+Workload (seeded, synthetic; the reference's dataset is not available):
+Chung-Lu power-law graph (exponent 2.1), 2^20 vertices, 2^24 undirected
+edges (10% withheld for re-insertion), 16 Zipf(1.2) labels; three 8-vertex
+random-walk queries (tree, one cycle, 14 edges); batches of 4096 updates,
+50% inserts from the withheld pool, 50% deletes of live edges.
+
+A step is one update batch matched against the three queries.  Forms:
+  batched (default): one engine, all queries in one persistent launch;
+  plain: one engine per query, one launch per query (the reference's
+         one-query-per-process form).
+
+Prints one JSON line.  `value` = delta-matches per second of device time
+(updates already resident; H2D of the next batch is not in the kernels'
+event window); `e2e` = the same through the C ABI with host buffers (host
+prep, H2D, matching, D2H, canonical result assembly) on the wall clock.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(steps, warmup, scale):
+    import dsm_b200 as d
+    nb = steps + warmup
+    return d.Workload(2, scale_log2=scale, num_batches=nb)
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    import dsm_b200 as d
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    w = make_workload(args.steps, args.warmup, args.scale)
+    gen_s = time.time() - t0
+    batches = list(w.batches())
+    queries = w.queries
+
+    def new_engine(qs):
+        e = d.Engine(dev)
+        e.set_option(d.OPT_LIST, args.list)
+        e.load_graph_edges(w.nv, w.labels, w.edges)
+        return e, [e.register(q) for q in qs]
+
+    if args.form == "batched":
+        engines = [new_engine(queries)]
+    else:
+        engines = [new_engine([q]) for q in queries]
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MiB > L2
+
+    def step(b):
+        """One batch through every engine; device ms, wall ms, matches, stats deltas."""
+        dev_ms = wall_ms = match_ms = 0.0
+        matches = alg = launches = 0
+        h2d = d2h = 0
+        for e, qids in engines:
+            s0 = e.stats()
+            torch.cuda.synchronize()
+            tw = time.perf_counter()
+            r = e.run_batch(b)
+            wall_ms += (time.perf_counter() - tw) * 1e3
+            s1 = e.stats()
+            dev_ms += s1["last_batch_ms"]
+            match_ms += s1["last_match_ms"]
+            matches += int(r.counts.sum())
+            alg += s1["alg_bytes"] - s0["alg_bytes"]
+            launches += s1["kernel_launches"] - s0["kernel_launches"]
+            h2d += b.nbytes
+            d2h += r.tuples.nbytes + r.counts.nbytes + r.signs.nbytes
+        return dev_ms, wall_ms, match_ms, matches, alg, launches, h2d, d2h
+
+    for b in batches[:args.warmup]:
+        step(b)
+    rows = []
+    sampler = ClockSampler(dev)
+    if rank == 0:
+        sampler.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    for b in batches[args.warmup:args.warmup + args.steps]:
+        flush.zero_()
+        torch.cuda.synchronize()
+        rows.append(step(b))
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = sampler.stop() if rank == 0 else None
+    R = np.array([r[:6] for r in rows], dtype=np.float64)
+    dev_ms, wall_ms, match_ms = R[:, 0].sum(), R[:, 1].sum(), R[:, 2].sum()
+    matches = int(R[:, 3].sum())
+    alg = float(R[:, 4].sum())
+    launches = int(R[:, 5].sum())
+    h2d = int(sum(r[6] for r in rows) / len(rows))
+    d2h = int(sum(r[7] for r in rows) / len(rows))
+    if world > 1:
+        t = torch.tensor([dev_ms, wall_ms, matches], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+        sm = t.clone()
+        torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
+        dev_ms, wall_ms, matches = float(mx[0]), float(mx[1]), int(sm[2])
+    if rank != 0:
+        return None
+    peak, peak_kind = _peaks()
+    upd = sum(len(b) for b in batches[args.warmup:args.warmup + args.steps]) * world
+    lat = np.sort(R[:, 1])
+    achieved = alg / 1e9 / (match_ms / 1e3) if match_ms > 0 else 0.0
+    line = {
+        "metric": "delta_matches_per_sec",
+        "value": matches / (dev_ms / 1e3) if dev_ms > 0 else 0.0,
+        "unit": "matches/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded Chung-Lu graph, random-walk queries, generated update stream)",
+        "config": {"workload": f"config2: Chung-Lu gamma=2.1, |V|=2^{20 + args.scale}, |E|=2^{24 + args.scale}, "
+                               "16 Zipf(1.2) labels, three 8-vertex queries, batches of 4096 (50/50)",
+                   "form": args.form, "listing": bool(args.list), "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between timed batches"},
+        "updates_per_sec": upd / (dev_ms / 1e3) if dev_ms > 0 else 0.0,
+        "matches": matches,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "e2e": {"value": matches / (wall_ms / 1e3) if wall_ms > 0 else 0.0, "unit": "matches/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "updates_per_sec": upd / (wall_ms / 1e3) if wall_ms > 0 else 0.0},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_match", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "alg_bytes_per_step": alg / args.steps},
+        "clocks": clocks,
+        "gen_seconds": gen_s,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w, batches[args.warmup], args.cpu_sample)
+    return line
+
+
+def cpu_baseline(w, batch, sample):
+    """The oracle (CPU restatement, one thread) on the first `sample` updates
+    of the first timed batch for each query."""
+    from oracle import oracle as orc
+    ups = batch[:sample]
+    matches = 0
+    secs = 0.0
+    for q in w.queries:
+        st = orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs)
+        t = time.perf_counter()
+        s, c, _ = st.apply(ups, listed=True)
+        secs += time.perf_counter() - t
+        matches += int(c.sum())
+    return {"value": matches / secs if secs > 0 else 0.0, "unit": "matches/s", "cores": 1, "kind": "port",
+            "sample": f"first {len(ups)} updates of the first timed batch x {len(w.queries)} queries, listed",
+            "seconds": secs}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    w = make_workload(args.steps, args.warmup, args.scale)
+    batches = list(w.batches())
+    from oracle import oracle as orc
+    streams = [orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs) for q in w.queries]
+    per = []
+    for b in batches[args.warmup:args.warmup + args.steps]:
+        ups = b[:args.cpu_sample]
+        t = time.perf_counter()
+        m = 0
+        for st in streams:
+            m += int(st.apply(ups, listed=True)[1].sum())
+        per.append((time.perf_counter() - t, m, len(ups)))
+    secs = sum(p[0] for p in per)
+    matches = sum(p[1] for p in per)
+    v = matches / secs if secs > 0 else 0.0
+    return {"impl": "reference", "metric": "delta_matches_per_sec", "value": v, "unit": "matches/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / len(per) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": {"workload": "config2 (see ours)", "form": "plain, CPU"},
+            "cpu_baseline": {"value": v, "unit": "matches/s", "cores": 1, "kind": "port",
+                             "sample": f"first {args.cpu_sample} updates of each timed batch x 3 queries"},
+            "e2e": {"value": v, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--list", type=int, default=1)
+    ap.add_argument("--scale", type=int, default=0, help="log2 shrink of the graph (0 = config size)")
+    ap.add_argument("--cpu-sample", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        # CPU arm: rank 0 alone runs; other ranks exit without work
+        line = run_reference(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    pg = False
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = True
+    try:
+        line = run_ours(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if pg:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

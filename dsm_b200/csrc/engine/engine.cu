@@ -1,0 +1,665 @@
+// Engine object and the C ABI (include/dsm.h).
+//
+// One engine owns one CUDA stream on one device.  A batch runs as
+//   upload -> edge state -> union insert -> seeds -> matcher
+//   -> (regrow + rerun on result overflow) -> delete -> clear marks -> download
+// with the data graph, query descriptors and scratch resident in HBM.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../../include/dsm.h"
+#include "../host/dsm_host.h"
+#include "../host/query_plan.h"
+#include "engine_internal.h"
+#include "kernels.cuh"
+
+namespace dsm {
+
+const char *status_string(int s) {
+  switch (s) {
+    case DSM_OK: return "ok";
+    case DSM_ERR_PARSE: return "parse error";
+    case DSM_ERR_OOM: return "out of device memory budget";
+    case DSM_ERR_OVERFLOW: return "capacity overflow";
+    case DSM_ERR_TIMEOUT: return "bounded device wait timed out";
+    case DSM_ERR_LIMIT: return "input beyond supported limits";
+    case DSM_ERR_ARG: return "bad argument";
+    case DSM_ERR_CUDA: return "CUDA error";
+    case DSM_ERR_STATE: return "invalid state";
+    case DSM_ERR_NOT_FOUND: return "not found";
+  }
+  return "unknown status";
+}
+
+int Engine::fail(int code, const std::string &msg) {
+  last_error = msg;
+  return code;
+}
+
+int Engine::cuda_fail(cudaError_t e, const char *where) {
+  last_error = std::string(where) + ": " + cudaGetErrorString(e);
+  return DSM_ERR_CUDA;
+}
+
+#define CK(call)                                    \
+  do {                                              \
+    cudaError_t _e = (call);                        \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+int Engine::dalloc(DevBuf &b, size_t bytes) {
+  if (b.bytes >= bytes && b.ptr) return DSM_OK;
+  size_t grow = std::max(bytes, b.bytes + b.bytes / 2);
+  grow = (grow + 255) & ~(size_t)255;
+  if (bytes_in_use - b.bytes + grow > budget) {
+    grow = bytes;
+    if (bytes_in_use - b.bytes + grow > budget)
+      return fail(DSM_ERR_OOM, "device memory budget exhausted (" + std::to_string(bytes) + " bytes requested)");
+  }
+  if (b.ptr) {
+    cudaFree(b.ptr);
+    bytes_in_use -= b.bytes;
+    b.ptr = nullptr;
+    b.bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&b.ptr, grow);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(DSM_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  b.bytes = grow;
+  bytes_in_use += grow;
+  return DSM_OK;
+}
+
+void Engine::dfree(DevBuf &b) {
+  if (b.ptr) {
+    cudaFree(b.ptr);
+    bytes_in_use -= b.bytes;
+  }
+  b.ptr = nullptr;
+  b.bytes = 0;
+}
+
+int Engine::halloc(HostBuf &b, size_t bytes) {
+  if (b.bytes >= bytes && b.ptr) return DSM_OK;
+  size_t grow = std::max(bytes, b.bytes + b.bytes / 2);
+  if (b.ptr) cudaFreeHost(b.ptr);
+  b.ptr = nullptr;
+  b.bytes = 0;
+  CK(cudaMallocHost(&b.ptr, grow));
+  b.bytes = grow;
+  return DSM_OK;
+}
+
+Engine::~Engine() {
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  for (DevBuf *b : all_dev_bufs()) dfree(*b);
+  for (HostBuf *b : {&h_stage, &h_sched, &h_segcnt, &h_vtp, &h_out_seg, &h_out_tup})
+    if (b->ptr) cudaFreeHost(b->ptr);
+  for (auto &ev : ev_pool)
+    if (ev) cudaEventDestroy(ev);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+std::vector<DevBuf *> Engine::all_dev_bufs() {
+  std::vector<DevBuf *> v = {&d_lab, &d_adj, &d_cap, &d_arena, &d_arena_top, &d_qd, &d_orders,
+                             &d_pair_off, &d_pair_ent, &d_upd, &d_bkey, &d_bidx, &d_binfo, &d_gflag,
+                             &d_vtp, &d_dkey, &d_dhead, &d_dsel, &d_seeds, &d_sched, &d_jobs,
+                             &d_job_ready, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc};
+  for (auto &q : slots) v.push_back(&q.bitmap);
+  for (auto &q : slots) v.push_back(&q.filter_scratch);
+  return v;
+}
+
+int Engine::init(int dev, size_t mem_budget) {
+  device = dev;
+  int n = 0;
+  CK(cudaGetDeviceCount(&n));
+  if (dev < 0 || dev >= n) return fail(DSM_ERR_ARG, "no such CUDA device");
+  CK(cudaSetDevice(dev));
+  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  num_sms = prop.multiProcessorCount;
+  int clk_khz = 0;
+  cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, dev);
+  clock_khz = clk_khz > 0 ? clk_khz : 1965000;
+  size_t freeb = 0, totalb = 0;
+  CK(cudaMemGetInfo(&freeb, &totalb));
+  budget = mem_budget ? mem_budget : (freeb > (1ull << 30) ? freeb - (1ull << 30) : freeb / 2);
+  ev_pool.resize(8, nullptr);
+  for (auto &ev : ev_pool) CK(cudaEventCreate(&ev));
+  int per_sm = match_max_blocks_per_sm();
+  match_blocks_per_sm = std::max(1, std::min(per_sm, 4));
+  // small fixed buffers
+  if (int rc = dalloc(d_sched, sizeof(Sched))) return rc;
+  if (int rc = dalloc(d_arena_top, 256)) return rc;
+  if (int rc = dalloc(d_misc, 256)) return rc;
+  if (int rc = halloc(h_sched, sizeof(Sched) + 64)) return rc;
+  return DSM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Graph
+// ---------------------------------------------------------------------------
+int Engine::load_graph(uint32_t nv_, const uint32_t *labels, std::vector<uint64_t> &keys) {
+  std::lock_guard<std::mutex> lk(mu);
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));
+  for (uint32_t v = 0; v < nv_; ++v)
+    if (labels[v] & kTouchBit) return fail(DSM_ERR_LIMIT, "vertex label >= 2^31");
+  // canonical, deduplicated undirected edges
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  std::vector<uint32_t> deg(nv_, 0);
+  for (uint64_t k : keys) {
+    deg[k >> 32]++;
+    deg[(uint32_t)k]++;
+  }
+  // slack: capacity = deg + deg/8 + 4, rounded to 16 bytes
+  std::vector<uint32_t> cap(nv_);
+  std::vector<uint2> adj(nv_);
+  uint64_t off16 = 0;
+  for (uint32_t v = 0; v < nv_; ++v) {
+    cap[v] = (deg[v] + deg[v] / 8 + 4 + 3) & ~3u;
+    adj[v] = make_uint2((uint32_t)off16, 0);
+    off16 += cap[v] / 4;
+  }
+  if (off16 > 0xFFFFFFFFull) return fail(DSM_ERR_LIMIT, "graph too large for 32-bit run offsets");
+  uint64_t used_words = off16 * 4;
+  uint64_t arena_words = used_words + used_words / 4 + (1u << 20);
+  arena_words = (arena_words + 3) & ~3ull;
+  // fill runs on the host (pinned) and upload once
+  HostBuf stage;
+  if (int rc = halloc(stage, used_words * 4)) return rc;
+  uint32_t *h_arena = (uint32_t *)stage.ptr;
+  std::vector<uint32_t> fill(nv_, 0);
+  for (uint64_t k : keys) {
+    uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
+    h_arena[(uint64_t)adj[a].x * 4 + fill[a]++] = b;
+    h_arena[(uint64_t)adj[b].x * 4 + fill[b]++] = a;
+  }
+  for (uint32_t v = 0; v < nv_; ++v) {
+    uint32_t *run = h_arena + (uint64_t)adj[v].x * 4;
+    std::sort(run, run + deg[v]);
+    for (uint32_t i = deg[v]; i < cap[v]; ++i) run[i] = 0xFFFFFFFFu;
+    adj[v].y = deg[v];
+  }
+  int rc;
+  if ((rc = dalloc(d_lab, (size_t)nv_ * 4)) || (rc = dalloc(d_adj, (size_t)nv_ * 8)) ||
+      (rc = dalloc(d_cap, (size_t)nv_ * 4)) || (rc = dalloc(d_arena, arena_words * 4))) {
+    cudaFreeHost(stage.ptr);
+    return rc;
+  }
+  CK(cudaMemcpyAsync(d_lab.ptr, labels, (size_t)nv_ * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_adj.ptr, adj.data(), (size_t)nv_ * 8, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_cap.ptr, cap.data(), (size_t)nv_ * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_arena.ptr, h_arena, used_words * 4, cudaMemcpyHostToDevice, stream));
+  unsigned long long top = off16;
+  CK(cudaMemcpyAsync(d_arena_top.ptr, &top, 8, cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  cudaFreeHost(stage.ptr);
+  nv = nv_;
+  this->arena_words = arena_words;
+  arena_used16 = off16;
+  graph_entries = 2 * keys.size();
+  graph_loaded = true;
+  label_host.assign(labels, labels + nv_);
+  for (auto &q : slots) q.filter_dirty = true;
+  return DSM_OK;
+}
+
+DevGraph Engine::dev_graph() {
+  DevGraph g;
+  g.nv = nv;
+  g.lab = (uint32_t *)d_lab.ptr;
+  g.adj = (uint2 *)d_adj.ptr;
+  g.cap = (uint32_t *)d_cap.ptr;
+  g.arena = (uint32_t *)d_arena.ptr;
+  g.arena_words = arena_words;
+  g.arena_top = (unsigned long long *)d_arena_top.ptr;
+  return g;
+}
+
+int Engine::export_graph(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries) {
+  std::lock_guard<std::mutex> lk(mu);
+  if (!graph_loaded) return fail(DSM_ERR_STATE, "no graph loaded");
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));
+  std::vector<uint2> adj(nv);
+  CK(cudaMemcpy(adj.data(), d_adj.ptr, (size_t)nv * 8, cudaMemcpyDeviceToHost));
+  uint64_t total = 0;
+  for (uint32_t v = 0; v < nv; ++v) total += adj[v].y;
+  if (num_entries) *num_entries = total;
+  if (offsets) {
+    uint64_t k = 0;
+    for (uint32_t v = 0; v < nv; ++v) {
+      offsets[v] = (uint32_t)k;
+      k += adj[v].y;
+    }
+    offsets[nv] = (uint32_t)k;
+  }
+  if (nbrs) {
+    uint64_t k = 0;
+    for (uint32_t v = 0; v < nv; ++v) {
+      if (adj[v].y)
+        CK(cudaMemcpy(nbrs + k, (uint32_t *)d_arena.ptr + (uint64_t)adj[v].x * 4, (size_t)adj[v].y * 4,
+                      cudaMemcpyDeviceToHost));
+      k += adj[v].y;
+    }
+  }
+  return DSM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Queries
+// ---------------------------------------------------------------------------
+int Engine::register_query(const uint32_t *qoff, const uint32_t *qnbr, const uint32_t *qlab, uint32_t nq,
+                           uint32_t *qid) {
+  std::lock_guard<std::mutex> lk(mu);
+  QueryPlan plan;
+  std::string err;
+  int rc = plan_query(nq, qoff, qnbr, qlab, plan, err);
+  if (rc) return fail(rc, err);
+  // admission: descriptor + filter bitmaps + encodings
+  size_t foot = sizeof(QDev) + plan.orders.size() * sizeof(OrderRec);
+  if (graph_loaded) foot += (size_t)nq * ((nv + 31) / 32) * 4 + (size_t)nv * plan.enc_words * 4 + (size_t)nv * nq * 4;
+  if (bytes_in_use + foot > budget)
+    return fail(DSM_ERR_OOM, "query admission: footprint " + std::to_string(foot) + " bytes exceeds the budget");
+  uint32_t id = (uint32_t)slots.size();
+  for (uint32_t i = 0; i < slots.size(); ++i)
+    if (!slots[i].live) {
+      id = i;
+      break;
+    }
+  if (id == slots.size()) slots.emplace_back();
+  if (id >= (1u << 23)) return fail(DSM_ERR_LIMIT, "too many queries");
+  Slot &s = slots[id];
+  s.live = true;
+  s.plan = std::move(plan);
+  s.filter_dirty = true;
+  queries_dirty = true;
+  *qid = id;
+  return DSM_OK;
+}
+
+int Engine::retire_query(uint32_t qid) {
+  std::lock_guard<std::mutex> lk(mu);
+  if (qid >= slots.size() || !slots[qid].live) return fail(DSM_ERR_NOT_FOUND, "no such query");
+  Slot &s = slots[qid];
+  s.live = false;
+  dfree(s.bitmap);
+  dfree(s.filter_scratch);
+  s.plan = QueryPlan();
+  queries_dirty = true;
+  return DSM_OK;
+}
+
+int Engine::sync_queries() {
+  if (!queries_dirty) return DSM_OK;
+  std::vector<QDev> qd(std::max<size_t>(slots.size(), 1));
+  std::vector<OrderRec> orders;
+  std::vector<std::vector<uint32_t>> buckets(32 * 32);
+  live_ids.clear();
+  max_width = 0;
+  for (uint32_t id = 0; id < slots.size(); ++id) {
+    Slot &s = slots[id];
+    if (!s.live) continue;
+    QDev &d = qd[id];
+    std::memset(&d, 0, sizeof(d));
+    d.nq = s.plan.nq;
+    d.order_base = (uint32_t)orders.size();
+    d.n_orders = (uint32_t)s.plan.orders.size();
+    d.local = (uint32_t)live_ids.size();
+    for (uint32_t u = 0; u < s.plan.nq; ++u) d.label[u] = s.plan.labels[u];
+    d.bitmap = nullptr;
+    d.col_len = (nv + 31) / 32;
+    for (size_t o = 0; o < s.plan.orders.size(); ++o) {
+      OrderRec r;
+      std::memcpy(&r, &s.plan.orders[o], sizeof(r));
+      orders.push_back(r);
+      uint32_t u = s.plan.oedges[o].first, v = s.plan.oedges[o].second;
+      buckets[s.plan.labels[u] * 32 + s.plan.labels[v]].push_back((id << 8) | (uint32_t)o);
+    }
+    live_ids.push_back(id);
+    max_width = std::max(max_width, s.plan.nq);
+  }
+  std::vector<uint32_t> pair_off(32 * 32 + 1, 0), pair_ent;
+  max_bucket = 0;
+  for (size_t b = 0; b < buckets.size(); ++b) {
+    pair_off[b + 1] = pair_off[b] + (uint32_t)buckets[b].size();
+    pair_ent.insert(pair_ent.end(), buckets[b].begin(), buckets[b].end());
+    max_bucket = std::max<uint32_t>(max_bucket, (uint32_t)buckets[b].size());
+  }
+  if (pair_ent.empty()) pair_ent.push_back(0);
+  if (orders.empty()) orders.emplace_back();
+  int rc;
+  if ((rc = dalloc(d_qd, qd.size() * sizeof(QDev))) || (rc = dalloc(d_orders, orders.size() * sizeof(OrderRec))) ||
+      (rc = dalloc(d_pair_off, pair_off.size() * 4)) || (rc = dalloc(d_pair_ent, pair_ent.size() * 4)))
+    return rc;
+  qd_host = qd;
+  CK(cudaMemcpyAsync(d_orders.ptr, orders.data(), orders.size() * sizeof(OrderRec), cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_pair_off.ptr, pair_off.data(), pair_off.size() * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_pair_ent.ptr, pair_ent.data(), pair_ent.size() * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  queries_dirty = false;
+  qd_dirty = true;
+  return DSM_OK;
+}
+
+int Engine::upload_qd() {
+  CK(cudaMemcpyAsync(d_qd.ptr, qd_host.data(), qd_host.size() * sizeof(QDev), cudaMemcpyHostToDevice, stream));
+  qd_dirty = false;
+  return DSM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches
+// ---------------------------------------------------------------------------
+int Engine::submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id) {
+  std::lock_guard<std::mutex> lk(mu);
+  if (!graph_loaded) return fail(DSM_ERR_STATE, "no graph loaded");
+  if (n >= (1u << 30)) return fail(DSM_ERR_LIMIT, "batch larger than 2^30 updates");
+  for (uint32_t i = 0; i < n; ++i)
+    if (ups[i].src >= nv || ups[i].dst >= nv) return fail(DSM_ERR_ARG, "update names a vertex >= num_v");
+  CK(cudaSetDevice(device));
+  auto res = std::make_unique<BatchResult>();
+  int rc = run_batch(ups, n, *res);
+  if (rc) return rc;
+  uint64_t id = next_batch_id++;
+  res->id = id;
+  results[id] = std::move(res);
+  *batch_id = id;
+  return DSM_OK;
+}
+
+int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
+  if (int rc = sync_queries()) return rc;
+  auto t_host0 = std::chrono::steady_clock::now();
+  const uint32_t nq_live = (uint32_t)live_ids.size();
+  // ---- host prep: sorted undirected keys and sorted directed pairs
+  std::vector<std::pair<uint64_t, uint32_t>> und;
+  und.reserve(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t a = ups[i].src, b = ups[i].dst;
+    if (a == b) continue;
+    uint64_t k = a < b ? ((uint64_t)a << 32) | b : ((uint64_t)b << 32) | a;
+    und.push_back({k, i});
+  }
+  std::sort(und.begin(), und.end());
+  const uint32_t m = (uint32_t)und.size();
+  std::vector<uint64_t> dir;
+  dir.reserve(2 * (size_t)m);
+  for (auto &e : und) {
+    uint32_t a = (uint32_t)(e.first >> 32), b = (uint32_t)e.first;
+    dir.push_back(((uint64_t)a << 32) | b);
+    dir.push_back(((uint64_t)b << 32) | a);
+  }
+  std::sort(dir.begin(), dir.end());
+  std::vector<uint32_t> dhead;
+  for (size_t j = 0; j < dir.size(); ++j)
+    if (j == 0 || (dir[j] >> 32) != (dir[j - 1] >> 32)) dhead.push_back((uint32_t)j);
+  const uint32_t ngroups = (uint32_t)dhead.size();
+  dhead.push_back((uint32_t)dir.size());
+
+  // ---- staging (pinned) and device buffers
+  const size_t up_bytes = (size_t)n * 16, bk_bytes = (size_t)m * 8, bi_bytes = (size_t)m * 4,
+               dk_bytes = dir.size() * 8, dh_bytes = dhead.size() * 4;
+  const size_t stage_bytes = up_bytes + bk_bytes + bi_bytes + dk_bytes + dh_bytes + 64;
+  int rc;
+  if ((rc = halloc(h_stage, stage_bytes))) return rc;
+  const size_t nn = std::max<uint32_t>(n, 1), mm = std::max<uint32_t>(m, 1), dd = std::max<size_t>(dir.size(), 1);
+  const unsigned long long seed_cap = (unsigned long long)nn * std::max<uint32_t>(max_bucket, 1);
+  const size_t nseg = (size_t)std::max<uint32_t>(nq_live, 1) * nn;
+  if ((rc = dalloc(d_upd, nn * 16)) || (rc = dalloc(d_bkey, mm * 8)) || (rc = dalloc(d_bidx, mm * 4)) ||
+      (rc = dalloc(d_binfo, mm * 4)) || (rc = dalloc(d_gflag, mm)) || (rc = dalloc(d_vtp, nn * 4)) ||
+      (rc = dalloc(d_dkey, dd * 8)) || (rc = dalloc(d_dhead, (dd + 1) * 4)) || (rc = dalloc(d_dsel, dd * 4)) ||
+      (rc = dalloc(d_seeds, seed_cap * 16)) || (rc = dalloc(d_segcnt, nseg * 8)))
+    return rc;
+  if (!d_jobs.ptr) {
+    if ((rc = dalloc(d_jobs, (size_t)job_cap * sizeof(JobRec))) || (rc = dalloc(d_job_ready, (size_t)job_cap * 4)))
+      return rc;
+    CK(cudaMemsetAsync(d_job_ready.ptr, 0, (size_t)job_cap * 4, stream));
+  }
+  if (list_mode) {
+    size_t cap = std::max<uint64_t>(result_cap, 1024);
+    if ((rc = dalloc(d_out_seg, cap * 4)) || (rc = dalloc(d_out_tup, cap * std::max<uint32_t>(max_width, 1) * 4)))
+      return rc;
+  }
+  char *st = (char *)h_stage.ptr;
+  size_t o_up = 0, o_bk = up_bytes, o_bi = o_bk + bk_bytes, o_dk = o_bi + bi_bytes, o_dh = o_dk + dk_bytes;
+  std::memcpy(st + o_up, ups, up_bytes);
+  for (uint32_t j = 0; j < m; ++j) {
+    ((uint64_t *)(st + o_bk))[j] = und[j].first;
+    ((uint32_t *)(st + o_bi))[j] = und[j].second;
+  }
+  std::memcpy(st + o_dk, dir.data(), dk_bytes);
+  std::memcpy(st + o_dh, dhead.data(), dh_bytes);
+  auto t_host1 = std::chrono::steady_clock::now();
+  R.host_prep_ms = std::chrono::duration<double, std::milli>(t_host1 - t_host0).count();
+
+  cudaEvent_t ev0 = ev_pool[0], ev_upd = ev_pool[1], ev_m0 = ev_pool[2], ev_m1 = ev_pool[3], ev_end = ev_pool[4];
+  CK(cudaEventRecord(ev0, stream));
+  if (n) CK(cudaMemcpyAsync(d_upd.ptr, st + o_up, up_bytes, cudaMemcpyHostToDevice, stream));
+  if (m) {
+    CK(cudaMemcpyAsync(d_bkey.ptr, st + o_bk, bk_bytes, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d_bidx.ptr, st + o_bi, bi_bytes, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d_dkey.ptr, st + o_dk, dk_bytes, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d_dhead.ptr, st + o_dh, dh_bytes, cudaMemcpyHostToDevice, stream));
+  }
+  CK(cudaMemsetAsync(d_vtp.ptr, 0xFF, nn * 4, stream));
+  CK(cudaMemsetAsync(d_sched.ptr, 0, sizeof(Sched), stream));
+  CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
+  CK(cudaMemsetAsync(d_misc.ptr, 0, 256, stream));
+  if (qd_dirty)
+    if ((rc = upload_qd())) return rc;
+
+  DevGraph g = dev_graph();
+  unsigned int *d_err = (unsigned int *)d_misc.ptr;
+  unsigned long long *d_reloc = (unsigned long long *)((char *)d_misc.ptr + 8);
+  EdgeStateArgs es{g, (const uint4 *)d_upd.ptr, (const unsigned long long *)d_bkey.ptr,
+                   (const uint32_t *)d_bidx.ptr, m, n, (uint32_t *)d_binfo.ptr, (uint8_t *)d_gflag.ptr,
+                   (uint32_t *)d_vtp.ptr};
+  launch_edge_state(es, stream);
+  stats.kernel_launches += (m > 0) + (ngroups > 0) + (nq_live > 0 && n > 0) + 1;  // + seeds, sched init
+  AdjUpdateArgs au{g, (const unsigned long long *)d_dkey.ptr, (const uint32_t *)d_dhead.ptr, ngroups,
+                   (const unsigned long long *)d_bkey.ptr, (const uint8_t *)d_gflag.ptr, m,
+                   (uint32_t *)d_dsel.ptr, d_err, d_reloc};
+  launch_adj_insert(au, stream);
+  CK(cudaEventRecord(ev_upd, stream));
+
+  // filters (per query, on the union graph)
+  if ((rc = run_filters())) return rc;
+
+  SeedArgs sa{g, (const uint4 *)d_upd.ptr, (const uint32_t *)d_vtp.ptr, n, (const uint32_t *)d_pair_off.ptr,
+              (const uint32_t *)d_pair_ent.ptr, (const QDev *)d_qd.ptr, (const OrderRec *)d_orders.ptr,
+              (uint4 *)d_seeds.ptr, seed_cap, (Sched *)d_sched.ptr};
+  if (nq_live) launch_seeds(sa, stream);
+  launch_sched_init((Sched *)d_sched.ptr, seed_cap, stream);
+
+  MatchArgs ma;
+  ma.g = g;
+  ma.bt = DevBatchEdges{(const unsigned long long *)d_bkey.ptr, (const uint32_t *)d_binfo.ptr, m};
+  ma.vtp = (const uint32_t *)d_vtp.ptr;
+  ma.n = n;
+  ma.qd = (const QDev *)d_qd.ptr;
+  ma.orders = (const OrderRec *)d_orders.ptr;
+  ma.seeds = (const uint4 *)d_seeds.ptr;
+  ma.sc = (Sched *)d_sched.ptr;
+  ma.jobs = (JobRec *)d_jobs.ptr;
+  ma.job_ready = (uint32_t *)d_job_ready.ptr;
+  ma.job_cap = job_cap;
+  ma.W = std::max<uint32_t>(max_width, 1);
+  ma.seg_count = (unsigned long long *)d_segcnt.ptr;
+  ma.list = list_mode;
+  ma.donate = donate;
+  ma.timeout_cycles = (long long)timeout_ms * (long long)clock_khz;
+  const int blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
+  Sched sc;
+  for (int attempt = 0;; ++attempt) {
+    ma.epoch = ++epoch;
+    ma.out_seg = (uint32_t *)d_out_seg.ptr;
+    ma.out_tup = (uint32_t *)d_out_tup.ptr;
+    ma.cap = list_mode ? d_out_seg.bytes / 4 : 0;
+    if (list_mode) ma.cap = std::min<unsigned long long>(ma.cap, d_out_tup.bytes / 4 / ma.W);
+    CK(cudaEventRecord(ev_m0, stream));
+    if (nq_live) {
+      launch_match(ma, blocks, stream);
+      ++stats.kernel_launches;
+    }
+    CK(cudaEventRecord(ev_m1, stream));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_sched.ptr, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    std::memcpy(&sc, h_sched.ptr, sizeof(Sched));
+    if (sc.error & kErrTimeout) return fail(DSM_ERR_TIMEOUT, "matcher: a bounded wait gave up");
+    if (sc.error & kErrSeeds) return fail(DSM_ERR_OVERFLOW, "seed table overflow");
+    if (!list_mode || sc.out_count <= ma.cap) break;
+    if (attempt >= 2) return fail(DSM_ERR_OVERFLOW, "result table kept overflowing");
+    // grow to the exact count and run the matcher again on the same union graph
+    ++stats.result_regrows;
+    result_cap = sc.out_count + sc.out_count / 8 + 1024;
+    if ((rc = dalloc(d_out_seg, result_cap * 4)) || (rc = dalloc(d_out_tup, result_cap * ma.W * 4))) return rc;
+    Sched reset;
+    std::memset(&reset, 0, sizeof(reset));
+    reset.nseeds = sc.nseeds;
+    reset.outstanding = sc.nseeds;
+    CK(cudaMemcpyAsync(d_sched.ptr, &reset, sizeof(reset), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  unsigned int err_host[4] = {0, 0, 0, 0};
+  unsigned long long reloc = 0;
+  // ---- deletions, marks, results
+  launch_adj_delete(au, stream);
+  launch_clear_touch(g, (const uint4 *)d_upd.ptr, n, stream);
+  stats.kernel_launches += (ngroups > 0) + (n > 0);
+  CK(cudaEventRecord(ev_end, stream));
+  size_t cnt = list_mode ? (size_t)sc.out_count : 0;
+  if ((rc = halloc(h_segcnt, nseg * 8)) || (rc = halloc(h_vtp, nn * 4))) return rc;
+  if (cnt) {
+    if ((rc = halloc(h_out_seg, cnt * 4)) || (rc = halloc(h_out_tup, cnt * ma.W * 4))) return rc;
+    CK(cudaMemcpyAsync(h_out_seg.ptr, d_out_seg.ptr, cnt * 4, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(h_out_tup.ptr, d_out_tup.ptr, cnt * ma.W * 4, cudaMemcpyDeviceToHost, stream));
+  }
+  CK(cudaMemcpyAsync(h_segcnt.ptr, d_segcnt.ptr, nseg * 8, cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(h_vtp.ptr, d_vtp.ptr, nn * 4, cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(err_host, d_misc.ptr, 16, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  std::memcpy(&reloc, (char *)err_host + 8, 8);
+  if (err_host[0] & kErrArena) return fail(DSM_ERR_OOM, "adjacency arena full (relocation failed)");
+  float ms_total = 0, ms_match = 0, ms_upd = 0;
+  cudaEventElapsedTime(&ms_total, ev0, ev_end);
+  cudaEventElapsedTime(&ms_match, ev_m0, ev_m1);
+  cudaEventElapsedTime(&ms_upd, ev0, ev_upd);
+
+  // ---- assemble the result view: counts, offsets, canonical order
+  R.n = n;
+  R.qids = live_ids;
+  R.widths.clear();
+  for (uint32_t id : live_ids) R.widths.push_back(slots[id].plan.nq);
+  R.signs.assign(n, 0);
+  const uint32_t *vtp = (const uint32_t *)h_vtp.ptr;
+  for (uint32_t i = 0; i < n; ++i)
+    if (vtp[i] != kNoView) R.signs[i] = ups[i].op ? 1 : -1;
+  R.counts.assign((size_t)nq_live * n, 0);
+  const unsigned long long *segc = (const unsigned long long *)h_segcnt.ptr;
+  for (size_t s = 0; s < (size_t)nq_live * n; ++s) R.counts[s] = segc[s];
+  R.offsets.assign((size_t)nq_live * n + 1, 0);
+  for (uint32_t ql = 0; ql < nq_live; ++ql)
+    for (uint32_t i = 0; i < n; ++i) {
+      size_t s = (size_t)ql * n + i;
+      R.offsets[s + 1] = R.offsets[s] + R.counts[s] * R.widths[ql];
+    }
+  R.listed = list_mode;
+  R.tuples.clear();
+  if (list_mode) {
+    R.tuples.resize(R.offsets.back());
+    std::vector<uint64_t> cur(R.offsets.begin(), R.offsets.end() - 1);
+    const uint32_t *hs = (const uint32_t *)h_out_seg.ptr, *ht = (const uint32_t *)h_out_tup.ptr;
+    for (size_t r = 0; r < cnt; ++r) {
+      uint32_t s = hs[r];
+      uint32_t w = R.widths[s / n];
+      std::memcpy(&R.tuples[cur[s]], ht + r * ma.W, w * 4);
+      cur[s] += w;
+    }
+    if (sort_results) {
+      for (size_t s = 0; s < (size_t)nq_live * n; ++s) {
+        size_t c = R.counts[s];
+        if (c < 2) continue;
+        uint32_t w = R.widths[s / n];
+        uint32_t *base = &R.tuples[R.offsets[s]];
+        std::vector<uint32_t> idx(c);
+        for (size_t i = 0; i < c; ++i) idx[i] = (uint32_t)i;
+        std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+          return std::lexicographical_compare(base + (size_t)x * w, base + (size_t)x * w + w, base + (size_t)y * w,
+                                              base + (size_t)y * w + w);
+        });
+        std::vector<uint32_t> tmp((size_t)c * w);
+        for (size_t i = 0; i < c; ++i) std::memcpy(&tmp[i * w], base + (size_t)idx[i] * w, w * 4);
+        std::memcpy(base, tmp.data(), tmp.size() * 4);
+      }
+    }
+  }
+  stats.batches++;
+  stats.updates += n;
+  stats.matches += sc.out_count;
+  stats.seeds += sc.nseeds;
+  stats.donations += sc.donations;
+  stats.steals += sc.steals;
+  stats.relocations += reloc;
+  stats.alg_bytes += sc.alg_bytes;
+  stats.last_batch_ms = ms_total;
+  stats.last_match_ms = ms_match;
+  stats.last_update_ms = ms_upd;
+  R.device_ms = ms_total;
+  R.match_ms = ms_match;
+  R.alg_bytes = sc.alg_bytes;
+  R.matches = sc.out_count;
+  return DSM_OK;
+}
+
+int Engine::run_filters() { return DSM_OK; }
+
+int Engine::query_filter(uint32_t, uint32_t *, uint32_t *) {
+  std::lock_guard<std::mutex> lk(mu);
+  return fail(DSM_ERR_STATE, "candidate filter not available");
+}
+
+int Engine::view(uint64_t id, dsm_result_view *v) {
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = results.find(id);
+  if (it == results.end()) return fail(DSM_ERR_NOT_FOUND, "no such batch (released?)");
+  BatchResult &R = *it->second;
+  v->batch_id = id;
+  v->num_updates = R.n;
+  v->num_queries = (uint32_t)R.qids.size();
+  v->qids = R.qids.data();
+  v->widths = R.widths.data();
+  v->signs = R.signs.data();
+  v->counts = R.counts.data();
+  v->offsets = R.offsets.data();
+  v->tuples = R.tuples.data();
+  v->listed = R.listed;
+  return DSM_OK;
+}
+
+int Engine::release(uint64_t id) {
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = results.find(id);
+  if (it == results.end()) return fail(DSM_ERR_NOT_FOUND, "no such batch");
+  results.erase(it);
+  return DSM_OK;
+}
+
+}  // namespace dsm

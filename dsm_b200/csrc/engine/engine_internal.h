@@ -1,0 +1,125 @@
+// Engine object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../../include/dsm.h"
+#include "../host/query_plan.h"
+#include "common.cuh"
+
+namespace dsm {
+
+const char *status_string(int s);
+
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+struct HostBuf {
+  void *ptr = nullptr;  // pinned
+  size_t bytes = 0;
+};
+
+struct Slot {
+  bool live = false;
+  QueryPlan plan;
+  DevBuf bitmap;          // nq x col_len candidate bitmaps
+  DevBuf filter_scratch;  // encodings, candidate lists
+  bool filter_dirty = true;
+};
+
+struct BatchResult {
+  uint64_t id = 0;
+  uint32_t n = 0;
+  std::vector<uint32_t> qids, widths;
+  std::vector<int8_t> signs;
+  std::vector<uint64_t> counts, offsets;
+  std::vector<uint32_t> tuples;
+  int listed = 1;
+  double device_ms = 0, match_ms = 0, host_prep_ms = 0;
+  uint64_t alg_bytes = 0, matches = 0;
+};
+
+struct Engine {
+  int device = 0;
+  size_t budget = 0;
+  size_t bytes_in_use = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  int clock_khz = 1965000;
+  int match_blocks_per_sm = 2;
+  std::mutex mu;
+  std::string last_error;
+  std::vector<cudaEvent_t> ev_pool;
+
+  // options
+  int list_mode = 1;
+  int filter_mode = 0;
+  int donate = 1;
+  int warps_per_sm = 0;
+  int64_t timeout_ms = 5000;
+  int label_quirk = 0;
+  int sort_results = 1;
+  uint64_t result_cap = 1 << 20;
+  uint32_t job_cap = 1 << 20;
+
+  // graph
+  bool graph_loaded = false;
+  uint32_t nv = 0;
+  uint64_t arena_words = 0, arena_used16 = 0, graph_entries = 0;
+  std::vector<uint32_t> label_host;
+  DevBuf d_lab, d_adj, d_cap, d_arena, d_arena_top;
+
+  // queries
+  std::vector<Slot> slots;
+  bool queries_dirty = true, qd_dirty = true;
+  std::vector<uint32_t> live_ids;
+  std::vector<QDev> qd_host;
+  uint32_t max_width = 0, max_bucket = 0;
+  DevBuf d_qd, d_orders, d_pair_off, d_pair_ent;
+
+  // batch scratch
+  DevBuf d_upd, d_bkey, d_bidx, d_binfo, d_gflag, d_vtp, d_dkey, d_dhead, d_dsel, d_seeds, d_sched, d_jobs,
+      d_job_ready, d_out_seg, d_out_tup, d_segcnt, d_misc;
+  HostBuf h_stage, h_sched, h_segcnt, h_vtp, h_out_seg, h_out_tup;
+  uint32_t epoch = 0;
+
+  // results
+  std::map<uint64_t, std::unique_ptr<BatchResult>> results;
+  uint64_t next_batch_id = 1;
+  dsm_stats stats{};
+
+  ~Engine();
+  int init(int device, size_t budget);
+  int fail(int code, const std::string &msg);
+  int cuda_fail(cudaError_t e, const char *where);
+  int dalloc(DevBuf &b, size_t bytes);
+  void dfree(DevBuf &b);
+  int halloc(HostBuf &b, size_t bytes);
+  std::vector<DevBuf *> all_dev_bufs();
+
+  int load_graph(uint32_t nv, const uint32_t *labels, std::vector<uint64_t> &keys);
+  DevGraph dev_graph();
+  int export_graph(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries);
+
+  int register_query(const uint32_t *qoff, const uint32_t *qnbr, const uint32_t *qlab, uint32_t nq, uint32_t *qid);
+  int retire_query(uint32_t qid);
+  int sync_queries();
+  int upload_qd();
+  int run_filters();
+  int query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);
+
+  int submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id);
+  int run_batch(const dsm_update *ups, uint32_t n, BatchResult &R);
+  int view(uint64_t id, dsm_result_view *v);
+  int release(uint64_t id);
+};
+
+}  // namespace dsm

@@ -1,0 +1,204 @@
+/*
+ * dsm.h -- C ABI of the B200 continuous subgraph matching engine.
+ *
+ * Plain pointers and sizes only.  Every call returns a status code
+ * (DSM_OK or one of DSM_ERR_*); nothing in the library calls exit().
+ * The reference (qxk152/DSM) exposes no library interface: its internal
+ * call boundaries, each named beside the entry point that replaces it, are
+ * process-global functions that exit() on error and keep their sizes in
+ * host globals and __constant__ symbols, so one query per process.
+ *
+ * One engine = one device, one CUDA stream, one data graph, any number of
+ * registered queries.  Calls on one engine are serialised internally (a
+ * mutex), so the ABI is thread-safe per engine.
+ */
+#ifndef DSM_H
+#define DSM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define DSM_OK 0
+#define DSM_ERR_PARSE 1    /* malformed text input */
+#define DSM_ERR_OOM 2      /* device memory budget or allocation exhausted */
+#define DSM_ERR_OVERFLOW 3 /* a result / queue capacity was exceeded and could not grow */
+#define DSM_ERR_TIMEOUT 4  /* a bounded device wait gave up */
+#define DSM_ERR_LIMIT 5    /* input beyond a supported size (query > 16 vertices, label >= 32, ...) */
+#define DSM_ERR_ARG 6      /* bad argument (null pointer, id out of range) */
+#define DSM_ERR_CUDA 7     /* CUDA runtime error */
+#define DSM_ERR_STATE 8    /* call not valid in the current state */
+#define DSM_ERR_NOT_FOUND 9
+
+typedef struct dsm_engine dsm_engine;
+
+/* One edge update, the reference's `change` (cpuGraph.h:13-18) plus its op
+ * letter: op 1 = 'a' (insert), 0 = 'd' (delete).  label is the data file's
+ * 4th field; labels stay fixed unless DSM_OPT_LABEL_QUIRK is set. */
+typedef struct dsm_update {
+  uint32_t op;
+  uint32_t src;
+  uint32_t dst;
+  uint32_t label;
+} dsm_update;
+
+/* ---- engine ----------------------------------------------------------- */
+/* Replaces main.cu:47-55 (device selection) and the process globals of
+ * globals.cu:4-74.  mem_budget = 0 means "free device memory minus 1 GiB". */
+int dsm_engine_create(int device, size_t mem_budget, dsm_engine **out);
+int dsm_engine_destroy(dsm_engine *e);
+const char *dsm_status_string(int status);
+/* Text of the last error on this engine ("" if none). */
+const char *dsm_last_error(dsm_engine *e);
+
+/* Options (dsm_engine_set_option). */
+#define DSM_OPT_LIST 1          /* 1: list embeddings (default); 0: counts only */
+#define DSM_OPT_FILTER 2        /* 0: labels only; 1: LDF+NLF; 2: cluster encoding (default) */
+#define DSM_OPT_RESULT_CAP 3    /* initial result capacity in tuples (grows on overflow) */
+#define DSM_OPT_WARPS_PER_SM 4  /* persistent matcher warps per SM (autotuned when 0) */
+#define DSM_OPT_DONATE 5        /* 0 disables work donation between warps */
+#define DSM_OPT_TIMEOUT_MS 6    /* bound on every device-side wait (default 5000) */
+#define DSM_OPT_LABEL_QUIRK 7   /* 1: an insert relabels both endpoints (cpuGraph.cpp:564) */
+#define DSM_OPT_SORT 8          /* 1: canonically sort each update's tuples (default) */
+int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
+int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
+
+/* ---- data graph ------------------------------------------------------- */
+/* Replaces readGraphToCPUDynamic's CSR hand-off + allocateMemGPU /
+ * copyGraphToGPU (io.cuh:19-31, io.cu:254-302).  The CSR may be in file
+ * order with duplicates; every entry (v, w) is read as the undirected edge
+ * {v, w}; self loops are dropped.  The device keeps sorted lists with slack. */
+int dsm_graph_load(dsm_engine *e, const uint32_t *offsets, const uint32_t *nbrs,
+                   const uint32_t *labels, uint32_t nv);
+/* Same, from an undirected edge list (ne pairs). */
+int dsm_graph_load_edges(dsm_engine *e, uint32_t nv, const uint32_t *labels, uint64_t ne,
+                         const uint32_t *edges);
+/* Current graph as a sorted CSR (offsets: nv+1 words; nbrs may be NULL to
+ * learn *num_entries first).  Parity hook for updateHostGraph
+ * (cpuGraph.cpp:521-607): the device lists must equal the set rebuild. */
+int dsm_graph_export(dsm_engine *e, uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries);
+int dsm_graph_info(dsm_engine *e, uint32_t *nv, uint64_t *num_entries, uint64_t *arena_words);
+
+/* ---- queries ---------------------------------------------------------- */
+/* Query CSR as read from a query file (file order, io.cu:181-189).  The
+ * host side runs decycle (decycle.cpp:6-135), the clustering plan of the
+ * cluster-encoding filter (filter.cu:23-392) and one matching order per
+ * ordered query edge (order.cpp:367-402, 647-676), then uploads a
+ * descriptor.  Admission: fails with DSM_ERR_OOM when the query's device
+ * footprint does not fit the engine's memory budget. */
+int dsm_query_register(dsm_engine *e, const uint32_t *q_offsets, const uint32_t *q_nbrs,
+                       const uint32_t *q_labels, uint32_t nq, uint32_t *qid);
+int dsm_query_retire(dsm_engine *e, uint32_t qid);
+/* Matching order for ordered query edge (u, v): order[p] = query vertex at
+ * position p; bn_mask[p] = positions < p adjacent to it (OrderCPU's
+ * v_orders / backward_neighbors, order.h:78-111). */
+int dsm_query_order(dsm_engine *e, uint32_t qid, uint32_t u, uint32_t v, uint32_t *order,
+                    uint32_t *bn_mask);
+/* Runs the candidate filter of query qid on the current graph and copies the
+ * per-u candidate bitmaps (nq * ceil(nv/32) words, u-major) -- the output of
+ * clusterFilter + compact (filter.cuh:119-137).  v_cand_us (nv words, may be
+ * NULL): bit u set when v passes LDF+NLF for u (d_v_candidate_us_). */
+int dsm_query_filter(dsm_engine *e, uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);
+
+/* Host only (no engine, no GPU): the plan the engine would build for a
+ * query.  orders / bn_masks: one row of nq words per ordered query edge, in
+ * CSR order; oedges: (u, v) per row; enc_pos_of_u: the encoding position
+ * whose bit is u's candidacy (filter.cu:1582-1609).  Outputs may be NULL. */
+int dsm_query_plan(const uint32_t *q_offsets, const uint32_t *q_nbrs, const uint32_t *q_labels,
+                   uint32_t nq, uint32_t *orders, uint32_t *bn_masks, uint32_t *oedges,
+                   uint32_t *num_oedges, uint32_t *enc_pos_of_u);
+
+/* ---- update batches -------------------------------------------------- */
+/* Replaces one iteration of the batch loop main.cu:152-347 (updateHostGraph,
+ * re-upload, re-filter, seeding, the matcher of gpu_match.cu/join.cu) for all
+ * registered queries at once.  Updates apply in array order with sequential
+ * semantics: an insert's positive matches are taken on the graph after it,
+ * a delete's negative matches on the graph before it.  Asynchronous: returns
+ * once the batch is queued on the engine stream. */
+int dsm_batch_submit(dsm_engine *e, const dsm_update *ups, uint32_t n, uint64_t *batch_id);
+/* Blocks until the batch's results are on the host. */
+int dsm_batch_wait(dsm_engine *e, uint64_t batch_id);
+
+typedef struct dsm_result_view {
+  uint64_t batch_id;
+  uint32_t num_updates;
+  uint32_t num_queries;
+  const uint32_t *qids;     /* [num_queries], ascending */
+  const uint32_t *widths;   /* [num_queries]: tuple width = query vertex count */
+  const int8_t *signs;      /* [num_updates]: +1 insert, -1 delete, 0 no-op update */
+  const uint64_t *counts;   /* [num_queries * num_updates], query-major */
+  const uint64_t *offsets;  /* [num_queries * num_updates + 1]: word offsets into tuples */
+  const uint32_t *tuples;   /* (f(0)..f(nq-1)) per embedding, each segment sorted */
+  int listed;               /* 0 when the batch ran with DSM_OPT_LIST = 0 */
+} dsm_result_view;
+/* Waits if needed; the view stays valid until dsm_batch_release. */
+int dsm_batch_results(dsm_engine *e, uint64_t batch_id, dsm_result_view *view);
+int dsm_batch_release(dsm_engine *e, uint64_t batch_id);
+
+/* ---- statistics ------------------------------------------------------- */
+typedef struct dsm_stats {
+  uint64_t batches;
+  uint64_t updates;
+  uint64_t matches;          /* total |P| + |N| emitted */
+  uint64_t seeds;            /* (update, ordered query edge) tasks */
+  uint64_t donations;        /* jobs handed from busy to idle warps */
+  uint64_t steals;           /* jobs taken from the shared queue */
+  uint64_t relocations;      /* adjacency lists moved for lack of slack */
+  uint64_t result_regrows;   /* result-buffer overflows retried */
+  uint64_t alg_bytes;        /* algorithmic bytes of the matcher (lists scanned, probes, output) */
+  double last_batch_ms;      /* device time of the last batch (events) */
+  double last_match_ms;      /* device time of the last matcher launch */
+  double last_filter_ms;
+  double last_update_ms;
+  double last_sort_ms;
+  uint64_t device_bytes_in_use;
+  uint64_t kernel_launches;  /* engine kernels launched so far */
+} dsm_stats;
+int dsm_engine_stats(dsm_engine *e, dsm_stats *s);
+
+/* ---- text formats and workloads (host only, no GPU needed) ------------ */
+typedef struct dsm_text dsm_text;
+/* readGraphToCPUDynamic (io.cu:122-252); is_query=1 stops after the graph. */
+int dsm_text_read(const char *path, int is_query, dsm_text **out, char *err, size_t err_len);
+void dsm_text_free(dsm_text *t);
+uint32_t dsm_text_nv(const dsm_text *t);
+uint32_t dsm_text_ne(const dsm_text *t);
+const uint32_t *dsm_text_labels(const dsm_text *t);
+const uint32_t *dsm_text_offsets(const dsm_text *t);
+const uint32_t *dsm_text_nbrs(const dsm_text *t);
+const uint32_t *dsm_text_edges(const dsm_text *t);
+uint32_t dsm_text_num_batches(const dsm_text *t);
+const uint32_t *dsm_text_batch_sizes(const dsm_text *t);
+uint32_t dsm_text_num_updates(const dsm_text *t);
+const dsm_update *dsm_text_updates(const dsm_text *t);
+
+typedef struct dsm_workload dsm_workload;
+/* Seeded synthetic workload for configs 1-5.  scale_log2 < 0 shrinks the
+ * graph by 2^-scale (vertices and edges), num_batches = 0 keeps the preset. */
+int dsm_workload_generate(int config, uint64_t seed, int scale_log2, uint32_t num_batches,
+                          dsm_workload **out);
+void dsm_workload_free(dsm_workload *w);
+uint32_t dsm_workload_nv(const dsm_workload *w);
+const uint32_t *dsm_workload_labels(const dsm_workload *w);
+uint64_t dsm_workload_num_edges(const dsm_workload *w);
+const uint32_t *dsm_workload_edges(const dsm_workload *w);
+uint32_t dsm_workload_num_queries(const dsm_workload *w);
+uint32_t dsm_workload_query_nv(const dsm_workload *w, uint32_t q);
+const uint32_t *dsm_workload_query_labels(const dsm_workload *w, uint32_t q);
+const uint32_t *dsm_workload_query_offsets(const dsm_workload *w, uint32_t q);
+const uint32_t *dsm_workload_query_nbrs(const dsm_workload *w, uint32_t q);
+uint32_t dsm_workload_num_batches(const dsm_workload *w);
+const uint32_t *dsm_workload_batch_sizes(const dsm_workload *w);
+uint32_t dsm_workload_num_updates(const dsm_workload *w);
+const dsm_update *dsm_workload_updates(const dsm_workload *w);
+/* Writes query_prefix<q>.in per query and data_path in the reference format. */
+int dsm_workload_write(const dsm_workload *w, const char *query_prefix, const char *data_path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSM_H */

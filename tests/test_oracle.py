@@ -1,0 +1,134 @@
+"""The CPU oracle pinned against the reference's fixture and against
+independent checks (brute force, count identities).  No GPU."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _kat():
+    with open(os.path.join(GOLD, "kat.json")) as f:
+        return json.load(f)
+
+
+def test_kat_reference_fixture():
+    kat = _kat()
+    q = orc.parse(os.path.join(GOLD, kat["query"]), True)
+    g = orc.parse(os.path.join(GOLD, kat["data"]), False)
+    assert q["nv"] == 5 and q["ne"] == 5 and g["nv"] == 11 and g["ne"] == 13
+    assert g["updates"].tolist() == kat["updates"] and g["batch_sizes"].tolist() == [1]
+    s = orc.Stream(g["nv"], g["labels"], g["edges"], q["labels"], q["offsets"], q["nbrs"])
+    assert s.count_all() == kat["count_before"]
+    signs, counts, tuples = s.apply(g["updates"])
+    assert signs.tolist() == kat["signs"]
+    assert tuples[0].tolist() == kat["positive"][0]
+    assert s.count_all() == kat["count_after"]
+
+
+def _random_graph(rng, nv, ne, nl):
+    labels = rng.integers(0, nl, nv).astype(np.uint32)
+    edges = set()
+    while len(edges) < ne:
+        a, b = rng.integers(0, nv, 2)
+        if a != b:
+            edges.add((min(a, b), max(a, b)))
+    return labels, np.array(sorted(edges), np.uint32)
+
+
+def _csr(nv, edges):
+    adj = [[] for _ in range(nv)]
+    for a, b in edges:
+        adj[a].append(b)
+        adj[b].append(a)
+    off = np.zeros(nv + 1, np.uint32)
+    nb = []
+    for v in range(nv):
+        nb += sorted(adj[v])
+        off[v + 1] = len(nb)
+    return off, np.array(nb, np.uint32)
+
+
+QUERIES = [
+    ([0, 0, 0], [(0, 1), (1, 2), (0, 2)]),                   # triangle
+    ([0, 1, 0, 1], [(0, 1), (1, 2), (2, 3)]),                 # path
+    ([0, 0, 1, 1], [(0, 1), (1, 2), (2, 3), (0, 3)]),         # 4-cycle
+    ([1, 0, 0, 0, 1], [(0, 1), (0, 2), (0, 3), (3, 4)]),      # tree
+    ([0, 0], [(0, 1)]),                                       # one edge
+]
+
+
+@pytest.mark.parametrize("qi", range(len(QUERIES)))
+def test_stream_matches_bruteforce(qi):
+    """Per-update sets vs brute-force counts before/after each update, on
+    graphs small enough to enumerate every injective map."""
+    import dsm_b200 as d
+    rng = np.random.default_rng(100 + qi)
+    ql, qe = QUERIES[qi]
+    q = d.Query.from_edges(ql, qe)
+    nv = 9
+    labels, edges = _random_graph(rng, nv, 16, 2)
+    st = orc.Stream(nv, labels, edges, q.labels, q.offsets, q.nbrs)
+    cur = set(map(tuple, edges.tolist()))
+
+    def bf():
+        off, nb = _csr(nv, sorted(cur))
+        return orc.bruteforce_count(q.labels, q.offsets, q.nbrs, nv, labels, off, nb)
+
+    before = bf()
+    assert st.count_all() == before
+    for step in range(40):
+        a, b = (int(x) for x in rng.integers(0, nv, 2))
+        op = int(rng.integers(0, 2))
+        signs, counts, tuples = st.apply(np.array([[op, a, b, labels[a]]]))
+        key = (min(a, b), max(a, b))
+        if a == b:
+            assert signs[0] == 0
+            continue
+        if op == 1 and key not in cur:
+            cur.add(key)
+            after = bf()
+            assert signs[0] == 1 and after - before == counts[0]
+        elif op == 0 and key in cur:
+            cur.discard(key)
+            after = bf()
+            assert signs[0] == -1 and before - after == counts[0]
+        else:
+            after = before
+            assert signs[0] == 0 and counts[0] == 0
+        # every tuple is an embedding that uses the updated edge
+        for t in tuples[0]:
+            assert len(set(t.tolist())) == len(t)
+            assert all(labels[t[u]] == q.labels[u] for u in range(q.nv))
+            used = {(min(t[x], t[y]), max(t[x], t[y])) for x, y in qe}
+            assert key in used
+        assert st.count_all() == after
+        before = after
+
+
+def test_count_identity_c1():
+    """Sum over a stream of |P| - |N| equals the change of the total count."""
+    import dsm_b200 as d
+    w = d.Workload(1)
+    q = w.queries[0]
+    st = orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs)
+    c0 = st.count_all()
+    ups = w.updates[:600]
+    signs, counts, _ = st.apply(ups, listed=False)
+    c1 = st.count_all()
+    delta = int((counts.astype(np.int64) * signs.astype(np.int64)).sum())
+    assert delta == int(c1) - int(c0)
+
+
+def test_parser_rejects_malformed(tmp_path):
+    p = tmp_path / "bad.in"
+    p.write_text("t 2 1\nv 0 0 1\nv 1 0 1\ne 0 5\n")
+    with pytest.raises(ValueError):
+        orc.parse(str(p), True)
+    p.write_text("t 2 1\nv 1 0 1\nv 0 0 1\ne 0 1\n")
+    with pytest.raises(ValueError):
+        orc.parse(str(p), True)
