@@ -142,6 +142,12 @@ def run_ours(args, rank, world):
             launches += s1["kernel_launches"] - s0["kernel_launches"]
             h2d += b.nbytes
             d2h += r.tuples.nbytes + r.counts.nbytes + r.signs.nbytes
+            if args.verbose:
+                print(f"  engine {qids}: dev {s1['last_batch_ms']:.2f} ms match {s1['last_match_ms']:.2f} ms "
+                      f"upd {s1['last_update_ms']:.2f} ms wall {(time.perf_counter() - tw) * 1e3:.1f} ms "
+                      f"matches {int(r.counts.sum())} per-query {r.counts.sum(axis=1).tolist()} "
+                      f"seeds {s1['seeds'] - s0['seeds']} donations {s1['donations'] - s0['donations']} "
+                      f"listed {r.listed}", file=sys.stderr, flush=True)
         return dev_ms, wall_ms, match_ms, matches, alg, launches, h2d, d2h
 
     for b in batches[:args.warmup]:
@@ -268,7 +274,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
-    ap.add_argument("--list", type=int, default=1)
+    # config 2's tree and one-cycle queries give 10^6..10^9 embeddings per batch
+    # at full size: the default measures exact counts (listing is covered by
+    # the parity tests); --list 1 lists and sorts them as well
+    ap.add_argument("--list", type=int, default=0)
+    ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--scale", type=int, default=0, help="log2 shrink of the graph (0 = config size)")
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -18,8 +18,8 @@ OK = 0
 ERR = {1: "PARSE", 2: "OOM", 3: "OVERFLOW", 4: "TIMEOUT", 5: "LIMIT", 6: "ARG", 7: "CUDA", 8: "STATE",
        9: "NOT_FOUND"}
 
-OPT_LIST, OPT_FILTER, OPT_RESULT_CAP, OPT_WARPS_PER_SM, OPT_DONATE, OPT_TIMEOUT_MS, OPT_LABEL_QUIRK, OPT_SORT = \
-    range(1, 9)
+OPT_LIST, OPT_FILTER, OPT_RESULT_CAP, OPT_WARPS_PER_SM, OPT_DONATE, OPT_TIMEOUT_MS, OPT_LABEL_QUIRK, OPT_SORT, \
+    OPT_LIST_LIMIT = range(1, 10)
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is not built; run `python dsm_b200/build.py`")

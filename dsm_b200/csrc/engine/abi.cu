@@ -76,6 +76,10 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
       E.label_quirk = 0;
       return DSM_OK;
     case DSM_OPT_SORT: E.sort_results = value ? 1 : 0; return DSM_OK;
+    case DSM_OPT_LIST_LIMIT:
+      if (value <= 0) return E.fail(DSM_ERR_ARG, "listing limit must be positive");
+      E.list_limit_bytes = (uint64_t)value;
+      return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");
 }
@@ -93,6 +97,7 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_TIMEOUT_MS: *value = E.timeout_ms; return DSM_OK;
     case DSM_OPT_LABEL_QUIRK: *value = E.label_quirk; return DSM_OK;
     case DSM_OPT_SORT: *value = E.sort_results; return DSM_OK;
+    case DSM_OPT_LIST_LIMIT: *value = (int64_t)E.list_limit_bytes; return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");
 }

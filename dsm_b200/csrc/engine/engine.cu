@@ -137,6 +137,7 @@ int Engine::init(int dev, size_t mem_budget) {
   size_t freeb = 0, totalb = 0;
   CK(cudaMemGetInfo(&freeb, &totalb));
   budget = mem_budget ? mem_budget : (freeb > (1ull << 30) ? freeb - (1ull << 30) : freeb / 2);
+  list_limit_bytes = std::min<uint64_t>(list_limit_bytes, budget / 4);
   ev_pool.resize(8, nullptr);
   for (auto &ev : ev_pool) CK(cudaEventCreate(&ev));
   int per_sm = match_max_blocks_per_sm();
@@ -506,6 +507,8 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   ma.timeout_cycles = (long long)timeout_ms * (long long)clock_khz;
   const int blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
   Sched sc;
+  int listed = list_mode;  // may drop to counts only for this batch
+  int match_rc = DSM_OK;   // a matcher failure still lets the batch's graph updates finish
   for (int attempt = 0;; ++attempt) {
     ma.epoch = ++epoch;
     ma.out_seg = (uint32_t *)d_out_seg.ptr;
@@ -522,10 +525,26 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
     CK(cudaMemcpyAsync(h_sched.ptr, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     std::memcpy(&sc, h_sched.ptr, sizeof(Sched));
-    if (sc.error & kErrTimeout) return fail(DSM_ERR_TIMEOUT, "matcher: a bounded wait gave up");
-    if (sc.error & kErrSeeds) return fail(DSM_ERR_OVERFLOW, "seed table overflow");
-    if (!list_mode || sc.out_count <= ma.cap) break;
-    if (attempt >= 2) return fail(DSM_ERR_OVERFLOW, "result table kept overflowing");
+    if (sc.error & kErrTimeout) {
+      match_rc = fail(DSM_ERR_TIMEOUT, "matcher: a bounded wait gave up");
+      break;
+    }
+    if (sc.error & kErrSeeds) {
+      match_rc = fail(DSM_ERR_OVERFLOW, "seed table overflow");
+      break;
+    }
+    if (!listed || sc.out_count <= ma.cap) break;
+    // the counts are complete (the matcher counts past the capacity); listing
+    // more than the limit downgrades this batch to counts only
+    if ((double)sc.out_count * (ma.W + 1) * 4.0 > (double)list_limit_bytes) {
+      listed = 0;
+      last_error = "batch listing exceeds the listing limit; returned counts only";
+      break;
+    }
+    if (attempt >= 2) {
+      match_rc = fail(DSM_ERR_OVERFLOW, "result table kept overflowing");
+      break;
+    }
     // grow to the exact count and run the matcher again on the same union graph
     ++stats.result_regrows;
     result_cap = sc.out_count + sc.out_count / 8 + 1024;
@@ -545,7 +564,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   launch_clear_touch(g, (const uint4 *)d_upd.ptr, n, stream);
   stats.kernel_launches += (ngroups > 0) + (n > 0);
   CK(cudaEventRecord(ev_end, stream));
-  size_t cnt = list_mode ? (size_t)sc.out_count : 0;
+  size_t cnt = (listed && match_rc == DSM_OK) ? (size_t)sc.out_count : 0;
   if ((rc = halloc(h_segcnt, nseg * 8)) || (rc = halloc(h_vtp, nn * 4))) return rc;
   if (cnt) {
     if ((rc = halloc(h_out_seg, cnt * 4)) || (rc = halloc(h_out_tup, cnt * ma.W * 4))) return rc;
@@ -558,6 +577,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   CK(cudaStreamSynchronize(stream));
   std::memcpy(&reloc, (char *)err_host + 8, 8);
   if (err_host[0] & kErrArena) return fail(DSM_ERR_OOM, "adjacency arena full (relocation failed)");
+  if (match_rc) return match_rc;
   float ms_total = 0, ms_match = 0, ms_upd = 0;
   cudaEventElapsedTime(&ms_total, ev0, ev_end);
   cudaEventElapsedTime(&ms_match, ev_m0, ev_m1);
@@ -579,11 +599,11 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   for (uint32_t ql = 0; ql < nq_live; ++ql)
     for (uint32_t i = 0; i < n; ++i) {
       size_t s = (size_t)ql * n + i;
-      R.offsets[s + 1] = R.offsets[s] + R.counts[s] * R.widths[ql];
+      R.offsets[s + 1] = R.offsets[s] + (listed ? R.counts[s] * R.widths[ql] : 0);
     }
-  R.listed = list_mode;
+  R.listed = listed;
   R.tuples.clear();
-  if (list_mode) {
+  if (listed) {
     R.tuples.resize(R.offsets.back());
     std::vector<uint64_t> cur(R.offsets.begin(), R.offsets.end() - 1);
     const uint32_t *hs = (const uint32_t *)h_out_seg.ptr, *ht = (const uint32_t *)h_out_tup.ptr;

@@ -69,6 +69,7 @@ struct Engine {
   int sort_results = 1;
   uint64_t result_cap = 1 << 20;
   uint32_t job_cap = 1 << 20;
+  uint64_t list_limit_bytes = 8ull << 30;  // beyond this a batch returns counts only
 
   // graph
   bool graph_loaded = false;

@@ -64,6 +64,8 @@ const char *dsm_last_error(dsm_engine *e);
 #define DSM_OPT_TIMEOUT_MS 6    /* bound on every device-side wait (default 5000) */
 #define DSM_OPT_LABEL_QUIRK 7   /* 1: an insert relabels both endpoints (cpuGraph.cpp:564) */
 #define DSM_OPT_SORT 8          /* 1: canonically sort each update's tuples (default) */
+#define DSM_OPT_LIST_LIMIT 9    /* bytes of tuples one batch may list; beyond it the batch
+                                   returns exact counts only and its view has listed = 0 */
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
 int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
 

@@ -60,14 +60,47 @@ def test_c1_stream_one_update_per_batch():
 
 
 @pytest.mark.parametrize("qi", [0, 1, 2])
-def test_c2_scaled_batches(qi):
+def test_c2_scaled_counts(qi):
     """Config 2 shape (Chung-Lu, Zipf labels, 8-vertex tree / cycle / dense
-    queries), scaled to 2^14 vertices, batches of 4096 mixed updates."""
+    queries), scaled to 2^14 vertices, batches of 4096 mixed updates: exact
+    per-update counts (count mode) and the graph after every batch."""
     w = d.Workload(2, scale_log2=-6, num_batches=2)
     q = w.queries[qi]
+    e, (qid,) = _fresh(None, w.nv, w.labels, w.edges, [q], OPT_LIST=0)
+    st = oracle_stream(w.nv, w.labels, w.edges, q)
+    run_stream(e, [qid], [st], list(w.batches()), check_graph_every=1, listed=False)
+    e.close()
+
+
+@pytest.mark.parametrize("qi", [0, 1, 2])
+def test_c2_scaled_listing(qi):
+    """Same workload, listed: every update's sorted embedding set, on the
+    longest prefix of the first batch whose listing stays below 2M tuples."""
+    w = d.Workload(2, scale_log2=-6, num_batches=1)
+    q = w.queries[qi]
+    b = next(w.batches())
+    n = len(b)
+    while n > 16:
+        c = oracle_stream(w.nv, w.labels, w.edges, q).apply(b[:n], listed=False)[1]
+        if c.sum() <= 2_000_000:
+            break
+        n //= 4
     e, (qid,) = _fresh(None, w.nv, w.labels, w.edges, [q])
     st = oracle_stream(w.nv, w.labels, w.edges, q)
-    run_stream(e, [qid], [st], list(w.batches()), check_graph_every=1)
+    run_stream(e, [qid], [st], [b[:n], b[n:n + 64]], check_graph_every=1)
+    e.close()
+
+
+def test_listing_limit_downgrades_to_counts():
+    w = d.Workload(1, scale_log2=-2)
+    b = np.concatenate(list(w.batches())[:400])
+    e, (qid,) = _fresh(None, w.nv, w.labels, w.edges, [w.queries[0]], OPT_LIST_LIMIT=64)
+    r = e.run_batch(b)
+    st = oracle_stream(w.nv, w.labels, w.edges, w.queries[0])
+    s, c, _ = st.apply(b, listed=False)
+    if c.sum() * (w.queries[0].nv + 1) * 4 > 64:
+        assert not r.listed
+    assert np.array_equal(r.counts[0], c)
     e.close()
 
 
