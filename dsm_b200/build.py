@@ -26,6 +26,7 @@ CXX_FLAGS = COMMON
 
 LIB_SOURCES = [
     "engine/kernels.cu",
+    "engine/match.cu",
     
     "engine/engine.cu",
     "engine/abi.cu",

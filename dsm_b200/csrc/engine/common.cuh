@@ -95,20 +95,27 @@ struct QDev {
 };
 
 // Scheduler state of one matcher launch (zeroed before each launch).
+// Counters that many warps touch sit on their own 128-byte lines, so that
+// waiting warps polling one of them do not slow the atomics of busy warps.
+struct alignas(128) SchedLine {
+  unsigned long long v;
+  unsigned long long pad[15];
+};
 struct Sched {
-  unsigned long long seed_next;
+  SchedLine seed_next;    // next seed to hand out
+  SchedLine outstanding;  // seeds + pushed jobs not finished yet
+  SchedLine push_cnt;     // job slots reserved by donors
+  SchedLine pop_cnt;      // tickets taken by idle warps (each waits for its slot)
+  SchedLine done;         // set once outstanding reached zero
+  SchedLine out_count;    // embeddings counted / slots reserved in the result table
+  SchedLine progress;     // heartbeat of busy warps (for the bounded waits)
+  // written rarely
   unsigned long long nseeds;
-  unsigned long long outstanding;  // seeds + pushed jobs not finished yet
-  unsigned long long push_cnt;
-  unsigned long long pop_cnt;
-  unsigned long long hungry;
-  unsigned long long progress;
-  unsigned long long out_count;
   unsigned long long donations;
   unsigned long long steals;
   unsigned long long alg_bytes;
   unsigned int error;
-  unsigned int pad;
+  unsigned int pad[7];
 };
 
 constexpr unsigned kErrTimeout = 1u;

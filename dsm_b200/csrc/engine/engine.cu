@@ -427,10 +427,14 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
       (rc = dalloc(d_dkey, dd * 8)) || (rc = dalloc(d_dhead, (dd + 1) * 4)) || (rc = dalloc(d_dsel, dd * 4)) ||
       (rc = dalloc(d_seeds, seed_cap * 16)) || (rc = dalloc(d_segcnt, nseg * 8)))
     return rc;
+  // donors check `push + k <= job_cap` and then reserve, so racing donors can
+  // overshoot by at most 32 slots each: one extra 32 slots per resident warp
+  const uint32_t job_slots = job_cap + 32u * (uint32_t)num_sms * 64u;
   if (!d_jobs.ptr) {
-    if ((rc = dalloc(d_jobs, (size_t)job_cap * sizeof(JobRec))) || (rc = dalloc(d_job_ready, (size_t)job_cap * 4)))
+    if ((rc = dalloc(d_jobs, (size_t)job_slots * sizeof(JobRec))) ||
+        (rc = dalloc(d_job_ready, (size_t)job_slots * 4)))
       return rc;
-    CK(cudaMemsetAsync(d_job_ready.ptr, 0, (size_t)job_cap * 4, stream));
+    CK(cudaMemsetAsync(d_job_ready.ptr, 0, (size_t)job_slots * 4, stream));
   }
   if (list_mode) {
     size_t cap = std::max<uint64_t>(result_cap, 1024);
@@ -500,6 +504,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   ma.jobs = (JobRec *)d_jobs.ptr;
   ma.job_ready = (uint32_t *)d_job_ready.ptr;
   ma.job_cap = job_cap;
+  ma.job_slots = job_slots;
   ma.W = std::max<uint32_t>(max_width, 1);
   ma.seg_count = (unsigned long long *)d_segcnt.ptr;
   ma.list = list_mode;
@@ -533,10 +538,10 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
       match_rc = fail(DSM_ERR_OVERFLOW, "seed table overflow");
       break;
     }
-    if (!listed || sc.out_count <= ma.cap) break;
+    if (!listed || sc.out_count.v <= ma.cap) break;
     // the counts are complete (the matcher counts past the capacity); listing
     // more than the limit downgrades this batch to counts only
-    if ((double)sc.out_count * (ma.W + 1) * 4.0 > (double)list_limit_bytes) {
+    if ((double)sc.out_count.v * (ma.W + 1) * 4.0 > (double)list_limit_bytes) {
       listed = 0;
       last_error = "batch listing exceeds the listing limit; returned counts only";
       break;
@@ -547,12 +552,13 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
     }
     // grow to the exact count and run the matcher again on the same union graph
     ++stats.result_regrows;
-    result_cap = sc.out_count + sc.out_count / 8 + 1024;
+    result_cap = sc.out_count.v + sc.out_count.v / 8 + 1024;
     if ((rc = dalloc(d_out_seg, result_cap * 4)) || (rc = dalloc(d_out_tup, result_cap * ma.W * 4))) return rc;
     Sched reset;
     std::memset(&reset, 0, sizeof(reset));
     reset.nseeds = sc.nseeds;
-    reset.outstanding = sc.nseeds;
+    reset.outstanding.v = sc.nseeds;
+    reset.done.v = sc.nseeds == 0;
     CK(cudaMemcpyAsync(d_sched.ptr, &reset, sizeof(reset), cudaMemcpyHostToDevice, stream));
     CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
     CK(cudaStreamSynchronize(stream));
@@ -564,7 +570,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   launch_clear_touch(g, (const uint4 *)d_upd.ptr, n, stream);
   stats.kernel_launches += (ngroups > 0) + (n > 0);
   CK(cudaEventRecord(ev_end, stream));
-  size_t cnt = (listed && match_rc == DSM_OK) ? (size_t)sc.out_count : 0;
+  size_t cnt = (listed && match_rc == DSM_OK) ? (size_t)sc.out_count.v : 0;
   if ((rc = halloc(h_segcnt, nseg * 8)) || (rc = halloc(h_vtp, nn * 4))) return rc;
   if (cnt) {
     if ((rc = halloc(h_out_seg, cnt * 4)) || (rc = halloc(h_out_tup, cnt * ma.W * 4))) return rc;
@@ -633,7 +639,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   }
   stats.batches++;
   stats.updates += n;
-  stats.matches += sc.out_count;
+  stats.matches += sc.out_count.v;
   stats.seeds += sc.nseeds;
   stats.donations += sc.donations;
   stats.steals += sc.steals;
@@ -645,7 +651,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   R.device_ms = ms_total;
   R.match_ms = ms_match;
   R.alg_bytes = sc.alg_bytes;
-  R.matches = sc.out_count;
+  R.matches = sc.out_count.v;
   return DSM_OK;
 }
 

@@ -68,7 +68,8 @@ struct MatchArgs {
   Sched *sc;
   JobRec *jobs;
   uint32_t *job_ready;
-  uint32_t job_cap;
+  uint32_t job_cap;    // donors stop reserving at this many slots
+  uint32_t job_slots;  // allocated slots: job_cap + room for racing reservations
   uint32_t epoch;
   uint32_t *out_seg;
   uint32_t *out_tup;
