@@ -628,6 +628,8 @@ struct Stream {
   std::vector<uint64_t> count;
   std::vector<uint32_t> tuples;
   uint64_t bytes = 0;
+  uint64_t work_budget = ~0ull;  // apply() stops enumerating once `bytes` passes this
+  uint32_t complete = 0;         // updates of the last apply with full results
 
   bool has_edge(uint32_t a, uint32_t b) const {
     const auto &l = adj[a];
@@ -638,6 +640,7 @@ struct Stream {
 void enumerate(const Stream &S, const Stream::Seed &sd, std::vector<uint32_t> &f, size_t p,
                bool list, uint64_t &cnt, std::vector<uint32_t> &out, uint64_t &bytes) {
   const uint32_t nq = S.nq;
+  if (bytes > S.work_budget) return;
   if (p == nq) {
     ++cnt;
     if (list) {
@@ -848,7 +851,31 @@ int orc_stream_apply(orc_stream *h, uint32_t n, const uint32_t *ups, int list) {
   S.count.assign(n, 0);
   S.tuples.clear();
   S.bytes = 0;
+  S.complete = n;
+  bool skipping = false;
   for (uint32_t i = 0; i < n; ++i) {
+    if (!skipping && S.bytes > S.work_budget) {
+      // out of budget: update i onward change the graph without enumeration
+      skipping = true;
+      S.complete = i;
+    }
+    if (skipping) {
+      uint32_t op = ups[4 * i], a = ups[4 * i + 1], b = ups[4 * i + 2];
+      if (a >= S.nv || b >= S.nv) return -1;
+      if (a == b) continue;
+      bool present = S.has_edge(a, b);
+      auto &la = S.adj[a], &lb = S.adj[b];
+      if (op == 1 && !present) {
+        la.insert(std::lower_bound(la.begin(), la.end(), b), b);
+        lb.insert(std::lower_bound(lb.begin(), lb.end(), a), a);
+        S.sign[i] = 1;
+      } else if (op == 0 && present) {
+        la.erase(std::lower_bound(la.begin(), la.end(), b));
+        lb.erase(std::lower_bound(lb.begin(), lb.end(), a));
+        S.sign[i] = -1;
+      }
+      continue;
+    }
     uint32_t op = ups[4 * i], a = ups[4 * i + 1], b = ups[4 * i + 2];
     if (a >= S.nv || b >= S.nv) return -1;
     if (a == b) continue;  // a self loop never lies on an embedding
@@ -869,9 +896,23 @@ int orc_stream_apply(orc_stream *h, uint32_t n, const uint32_t *ups, int list) {
       la.erase(std::lower_bound(la.begin(), la.end(), b));
       lb.erase(std::lower_bound(lb.begin(), lb.end(), a));
     }
+    if (S.bytes > S.work_budget && !skipping) {
+      skipping = true;  // update i's own count may be partial
+      S.complete = i;
+    }
   }
-  return 0;
+  if (S.complete < n && list) {
+    // drop tuples of updates past the complete prefix
+    uint64_t keep = 0;
+    for (uint32_t i = 0; i < S.complete; ++i) keep += S.count[i];
+    S.tuples.resize(keep * S.nq);
+  }
+  for (uint32_t i = S.complete; i < n; ++i) S.count[i] = 0;
+  return S.complete < n ? 1 : 0;
 }
+
+void orc_stream_set_budget(orc_stream *h, uint64_t bytes) { h->s.work_budget = bytes; }
+uint32_t orc_stream_complete(const orc_stream *h) { return h->s.complete; }
 
 int8_t orc_stream_sign(const orc_stream *s, uint32_t i) { return s->s.sign[i]; }
 uint64_t orc_stream_count(const orc_stream *s, uint32_t i) { return s->s.count[i]; }

@@ -97,6 +97,12 @@ void orc_stream_free(orc_stream *s);
 /* Apply n updates (4 words each: op, src, dst, label) one at a time.
  * list=0 counts only.  Results of this call replace the previous ones. */
 int orc_stream_apply(orc_stream *s, uint32_t n, const uint32_t *updates, int list);
+/* Work budget in algorithmic bytes per apply call.  Once passed, the call
+ * still applies every update to the graph but enumerates no further: the
+ * first orc_stream_complete() updates have full results, the rest have
+ * count 0, and apply returns 1.  Lets tests afford explosive updates. */
+void orc_stream_set_budget(orc_stream *s, uint64_t bytes);
+uint32_t orc_stream_complete(const orc_stream *s);
 int8_t orc_stream_sign(const orc_stream *s, uint32_t i);
 uint64_t orc_stream_count(const orc_stream *s, uint32_t i);
 /* Tuples of the last apply, concatenated in update order, nq words each. */

@@ -42,6 +42,8 @@ _sig("orc_cluster_filter", C.c_int, C.c_uint32, u32p, u32p, u32p, C.c_uint32, u3
 _sig("orc_stream_new", C.c_int, C.c_uint32, u32p, C.c_uint64, u32p, C.c_uint32, u32p, u32p, u32p, C.POINTER(P))
 _sig("orc_stream_free", None, P)
 _sig("orc_stream_apply", C.c_int, P, C.c_uint32, u32p, C.c_int)
+_sig("orc_stream_set_budget", None, P, C.c_uint64)
+_sig("orc_stream_complete", C.c_uint32, P)
 _sig("orc_stream_sign", C.c_int8, P, C.c_uint32)
 _sig("orc_stream_count", C.c_uint64, P, C.c_uint32)
 _sig("orc_stream_tuples", C.POINTER(C.c_uint32), P, C.POINTER(C.c_uint64))
@@ -147,8 +149,11 @@ class Stream:
         n = len(u) // 4
         if n == 0:
             return np.zeros(0, np.int8), np.zeros(0, np.uint64), []
-        if lib.orc_stream_apply(self._h, n, u, int(listed)):
+        rc = lib.orc_stream_apply(self._h, n, u, int(listed))
+        if rc not in (0, 1):
             raise ValueError("oracle apply failed")
+        # with a work budget, only the first `complete` updates have results
+        self.complete = lib.orc_stream_complete(self._h)
         signs = np.array([lib.orc_stream_sign(self._h, i) for i in range(n)], np.int8)
         counts = np.array([lib.orc_stream_count(self._h, i) for i in range(n)], np.uint64)
         if not listed:
@@ -161,6 +166,10 @@ class Stream:
             out.append(flat[pos:pos + int(c)])
             pos += int(c)
         return signs, counts, out
+
+    def set_budget(self, nbytes):
+        """Work budget (algorithmic bytes) of each later apply call."""
+        lib.orc_stream_set_budget(self._h, int(nbytes))
 
     def count_all(self):
         return lib.orc_stream_count_all(self._h)
