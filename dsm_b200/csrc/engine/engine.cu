@@ -538,14 +538,14 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
       match_rc = fail(DSM_ERR_OVERFLOW, "seed table overflow");
       break;
     }
-    if (!listed || sc.out_count.v <= ma.cap) break;
     // the counts are complete (the matcher counts past the capacity); listing
     // more than the limit downgrades this batch to counts only
-    if ((double)sc.out_count.v * (ma.W + 1) * 4.0 > (double)list_limit_bytes) {
+    if (listed && (double)sc.out_count.v * (ma.W + 1) * 4.0 > (double)list_limit_bytes) {
       listed = 0;
       last_error = "batch listing exceeds the listing limit; returned counts only";
       break;
     }
+    if (!listed || sc.out_count.v <= ma.cap) break;
     if (attempt >= 2) {
       match_rc = fail(DSM_ERR_OVERFLOW, "result table kept overflowing");
       break;
