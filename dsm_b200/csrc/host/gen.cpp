@@ -250,91 +250,102 @@ uint64_t capped_edge_count(const Adj &g, const std::vector<uint32_t> &labels, co
   return std::min(cnt, cap);
 }
 
-// Random-walk query: a walk from a random non-isolated vertex adds each newly
-// reached vertex with the walk edge that reached it (a spanning tree), then
-// `extra` further edges are drawn from the data edges induced on the sampled
+// Random-walk query: a walk from a random vertex adds each newly reached
+// vertex with the walk edge that reached it (a spanning tree), then `extra`
+// further edges are drawn from the data edges induced on the sampled
 // vertices.  Labels are copied.  Returns false when no sample was found.
 //
-// With max_mean > 0 a sample is accepted only when it is selective enough to
-// be listed: on a power-law graph a tree-like query through two hubs has
-// ~deg^k embeddings per update, which no engine can list.
-bool sample_query(const Adj &g, const std::vector<uint32_t> &labels, const std::vector<uint64_t> &probe,
-                  uint32_t nq, uint32_t extra, double max_mean, Rng &r, Query &q) {
+// With max_mean > 0 a sample must also be selective enough to be listed:
+// on a power-law graph a tree-like query through two hubs has ~deg^k
+// embeddings per update, which no engine can list.  The test counts the
+// embeddings through each probe edge (the workload's own update edges, in
+// random order), each capped at 10 x max_mean; a candidate passes when no
+// edge reaches the cap and the mean stays within max_mean.  Candidates are
+// drawn in tiers: tier t walks only over vertices whose label is not among
+// the t most frequent labels (the walk stays put when the step would leave
+// the allowed vertices), so later tiers copy rarer labels.  Each tier tries
+// kPerTier candidates; if no tier passes, the candidate with the smallest
+// capped total is returned.
+bool sample_query(const Adj &g, const std::vector<uint32_t> &labels, const std::vector<uint32_t> &label_rank,
+                  const std::vector<uint64_t> &probe, uint32_t nq, uint32_t extra, double max_mean, Rng &r,
+                  Query &q) {
   const uint32_t nv = (uint32_t)labels.size();
-  constexpr int kScored = 16;
+  const bool selective = max_mean > 0 && !probe.empty();
+  constexpr int kPerTier = 12;
+  const uint32_t nlabels = (uint32_t)label_rank.size();
+  const uint32_t tiers = selective ? std::max<uint32_t>(1, nlabels > 3 ? nlabels - 3 : 1) : 1;
   double best_total = 1e300;
   Query best;
-  int scored = 0;
-  for (int attempt = 0; attempt < 20000; ++attempt) {
-    uint32_t start = (uint32_t)r.below(nv);
-    if (g.deg(start) == 0) continue;
-    std::vector<uint32_t> vs{start};
-    std::vector<std::pair<uint32_t, uint32_t>> tree;
-    uint32_t cur = start;
-    for (uint32_t step = 0; step < 64 * nq && vs.size() < nq; ++step) {
-      uint32_t d = g.deg(cur);
-      if (d == 0) break;
-      uint32_t w = g.nbr[g.off[cur] + r.below(d)];
-      auto it = std::find(vs.begin(), vs.end(), w);
-      if (it == vs.end()) {
-        tree.push_back({(uint32_t)(std::find(vs.begin(), vs.end(), cur) - vs.begin()),
-                        (uint32_t)vs.size()});
-        vs.push_back(w);
+  for (uint32_t tier = 0; tier < tiers; ++tier) {
+    auto allowed = [&](uint32_t v) { return label_rank[labels[v]] >= tier; };
+    int scored = 0;
+    for (int attempt = 0; attempt < 4000 && scored < kPerTier; ++attempt) {
+      uint32_t start = (uint32_t)r.below(nv);
+      if (g.deg(start) == 0 || !allowed(start)) continue;
+      std::vector<uint32_t> vs{start};
+      std::vector<std::pair<uint32_t, uint32_t>> tree;
+      uint32_t cur = start;
+      for (uint32_t step = 0; step < 64 * nq && vs.size() < nq; ++step) {
+        uint32_t d = g.deg(cur);
+        if (d == 0) break;
+        uint32_t w = g.nbr[g.off[cur] + r.below(d)];
+        if (!allowed(w)) continue;
+        auto it = std::find(vs.begin(), vs.end(), w);
+        if (it == vs.end()) {
+          tree.push_back({(uint32_t)(std::find(vs.begin(), vs.end(), cur) - vs.begin()), (uint32_t)vs.size()});
+          vs.push_back(w);
+        }
+        cur = w;
       }
-      cur = w;
-    }
-    if (vs.size() < nq) continue;
-    std::vector<std::pair<uint32_t, uint32_t>> cand;
-    for (uint32_t i = 0; i < nq; ++i)
-      for (uint32_t j = i + 1; j < nq; ++j) {
-        bool in_tree = false;
-        for (auto &t : tree)
-          if ((t.first == i && t.second == j) || (t.first == j && t.second == i)) in_tree = true;
-        if (!in_tree && g.has(vs[i], vs[j])) cand.push_back({i, j});
+      if (vs.size() < nq) continue;
+      std::vector<std::pair<uint32_t, uint32_t>> cand;
+      for (uint32_t i = 0; i < nq; ++i)
+        for (uint32_t j = i + 1; j < nq; ++j) {
+          bool in_tree = false;
+          for (auto &t : tree)
+            if ((t.first == i && t.second == j) || (t.first == j && t.second == i)) in_tree = true;
+          if (!in_tree && g.has(vs[i], vs[j])) cand.push_back({i, j});
+        }
+      if (cand.size() < extra) continue;
+      shuffle(cand, r);
+      std::vector<std::pair<uint32_t, uint32_t>> edges = tree;
+      edges.insert(edges.end(), cand.begin(), cand.begin() + extra);
+      for (auto &e : edges)
+        if (e.first > e.second) std::swap(e.first, e.second);
+      std::sort(edges.begin(), edges.end());
+      q.nv = nq;
+      q.labels.resize(nq);
+      for (uint32_t i = 0; i < nq; ++i) q.labels[i] = labels[vs[i]];
+      q.edges.clear();
+      for (auto &e : edges) {
+        q.edges.push_back(e.first);
+        q.edges.push_back(e.second);
       }
-    if (cand.size() < extra) continue;
-    shuffle(cand, r);
-    std::vector<std::pair<uint32_t, uint32_t>> edges = tree;
-    edges.insert(edges.end(), cand.begin(), cand.begin() + extra);
-    for (auto &e : edges)
-      if (e.first > e.second) std::swap(e.first, e.second);
-    std::sort(edges.begin(), edges.end());
-    q.nv = nq;
-    q.labels.resize(nq);
-    for (uint32_t i = 0; i < nq; ++i) q.labels[i] = labels[vs[i]];
-    q.edges.clear();
-    for (auto &e : edges) {
-      q.edges.push_back(e.first);
-      q.edges.push_back(e.second);
+      q.build_csr();
+      if (!selective) return true;
+      ++scored;
+      const uint64_t cap = (uint64_t)(10 * max_mean) + 1;
+      const double budget = max_mean * (double)probe.size();
+      double total = 0;
+      bool pass = true;
+      for (uint64_t k : probe) {
+        uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
+        uint64_t c = capped_edge_count(g, labels, q, a, b, cap);
+        if (c < cap) c += capped_edge_count(g, labels, q, b, a, cap - c);
+        total += (double)c;
+        if (c >= cap || total > budget) {
+          pass = false;
+          if (total >= best_total) break;
+        }
+      }
+      if (pass) return true;
+      if (total < best_total) {
+        best_total = total;
+        best = q;
+      }
     }
-    q.build_csr();
-    if (max_mean <= 0 || probe.empty()) return true;
-    // Embeddings through each probe edge (the workload's own update edges,
-    // in random order), each capped at 50 x max_mean.  A candidate within
-    // budget (mean <= max_mean, no edge at the cap) is taken at once;
-    // otherwise the candidate with the smallest capped total is kept and,
-    // after kScored candidates, returned.  Scoring stops early once a
-    // candidate cannot beat the best one.
-    const uint64_t cap = (uint64_t)(10 * max_mean) + 1;
-    const double budget = max_mean * (double)probe.size();
-    double total = 0;
-    bool within = true;
-    for (uint64_t k : probe) {
-      uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
-      uint64_t c = capped_edge_count(g, labels, q, a, b, cap);
-      if (c < cap) c += capped_edge_count(g, labels, q, b, a, cap - c);
-      total += (double)c;
-      if (c >= cap || total > budget) within = false;
-      if (total >= best_total) break;
-    }
-    if (within) return true;
-    if (total < best_total) {
-      best_total = total;
-      best = q;
-    }
-    if (++scored >= kScored) break;
   }
-  if (scored > 0 && best_total < 1e300) {
+  if (best_total < 1e300) {
     q = best;
     return true;
   }
@@ -468,6 +479,16 @@ int generate_workload(const GenParams &p, Workload &w) {
   // shapes and per-query seeds are drawn in order; the samples themselves run
   // on all host threads (each query has its own stream, so the result does
   // not depend on the thread count)
+  // frequency rank of each label (0 = most frequent)
+  std::vector<uint32_t> label_rank(p.num_labels, 0);
+  {
+    std::vector<uint64_t> freq(p.num_labels, 0);
+    for (uint32_t l : w.labels) freq[l]++;
+    std::vector<uint32_t> ids(p.num_labels);
+    for (uint32_t l = 0; l < p.num_labels; ++l) ids[l] = l;
+    std::stable_sort(ids.begin(), ids.end(), [&](uint32_t x, uint32_t y) { return freq[x] > freq[y]; });
+    for (uint32_t k = 0; k < p.num_labels; ++k) label_rank[ids[k]] = k;
+  }
   const uint32_t nqs = p.num_queries;
   std::vector<uint32_t> q_nv(nqs), q_extra(nqs);
   std::vector<uint64_t> q_seed(nqs);
@@ -488,7 +509,8 @@ int generate_workload(const GenParams &p, Workload &w) {
   auto worker = [&]() {
     for (uint32_t qi; (qi = next.fetch_add(1)) < nqs;) {
       Rng rl(q_seed[qi]);
-      ok[qi] = sample_query(g, w.labels, probe, q_nv[qi], q_extra[qi], p.q_max_mean_matches, rl, w.queries[qi]);
+      ok[qi] = sample_query(g, w.labels, label_rank, probe, q_nv[qi], q_extra[qi], p.q_max_mean_matches, rl,
+                            w.queries[qi]);
     }
   };
   unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 32));
