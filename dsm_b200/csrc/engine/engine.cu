@@ -115,7 +115,7 @@ std::vector<DevBuf *> Engine::all_dev_bufs() {
   std::vector<DevBuf *> v = {&d_lab, &d_adj, &d_cap, &d_arena, &d_arena_top, &d_qd, &d_orders,
                              &d_pair_off, &d_pair_ent, &d_upd, &d_bkey, &d_bidx, &d_binfo, &d_gflag,
                              &d_vtp, &d_dkey, &d_dhead, &d_dsel, &d_seeds, &d_sched, &d_jobs,
-                             &d_job_ready, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc};
+                             &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc};
   for (auto &q : slots) v.push_back(&q.bitmap);
   for (auto &q : slots) v.push_back(&q.filter_scratch);
   return v;
@@ -427,14 +427,9 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
       (rc = dalloc(d_dkey, dd * 8)) || (rc = dalloc(d_dhead, (dd + 1) * 4)) || (rc = dalloc(d_dsel, dd * 4)) ||
       (rc = dalloc(d_seeds, seed_cap * 16)) || (rc = dalloc(d_segcnt, nseg * 8)))
     return rc;
-  // donors check `push + k <= job_cap` and then reserve, so racing donors can
-  // overshoot by at most 32 slots each: one extra 32 slots per resident warp
-  const uint32_t job_slots = job_cap + 32u * (uint32_t)num_sms * 64u;
   if (!d_jobs.ptr) {
-    if ((rc = dalloc(d_jobs, (size_t)job_slots * sizeof(JobRec))) ||
-        (rc = dalloc(d_job_ready, (size_t)job_slots * 4)))
+    if ((rc = dalloc(d_jobs, (size_t)job_ring * sizeof(JobRec))) || (rc = dalloc(d_job_seq, (size_t)job_ring * 8)))
       return rc;
-    CK(cudaMemsetAsync(d_job_ready.ptr, 0, (size_t)job_slots * 4, stream));
   }
   if (list_mode) {
     size_t cap = std::max<uint64_t>(result_cap, 1024);
@@ -490,7 +485,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
               (const uint32_t *)d_pair_ent.ptr, (const QDev *)d_qd.ptr, (const OrderRec *)d_orders.ptr,
               (uint4 *)d_seeds.ptr, seed_cap, (Sched *)d_sched.ptr};
   if (nq_live) launch_seeds(sa, stream);
-  launch_sched_init((Sched *)d_sched.ptr, seed_cap, stream);
+  launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream);
 
   MatchArgs ma;
   ma.g = g;
@@ -502,9 +497,8 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   ma.seeds = (const uint4 *)d_seeds.ptr;
   ma.sc = (Sched *)d_sched.ptr;
   ma.jobs = (JobRec *)d_jobs.ptr;
-  ma.job_ready = (uint32_t *)d_job_ready.ptr;
-  ma.job_cap = job_cap;
-  ma.job_slots = job_slots;
+  ma.job_seq = (unsigned long long *)d_job_seq.ptr;
+  ma.job_ring = job_ring;
   ma.W = std::max<uint32_t>(max_width, 1);
   ma.seg_count = (unsigned long long *)d_segcnt.ptr;
   ma.list = list_mode;
@@ -515,7 +509,6 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   int listed = list_mode;  // may drop to counts only for this batch
   int match_rc = DSM_OK;   // a matcher failure still lets the batch's graph updates finish
   for (int attempt = 0;; ++attempt) {
-    ma.epoch = ++epoch;
     ma.out_seg = (uint32_t *)d_out_seg.ptr;
     ma.out_tup = (uint32_t *)d_out_tup.ptr;
     ma.cap = list_mode ? d_out_seg.bytes / 4 : 0;
@@ -557,10 +550,10 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
     Sched reset;
     std::memset(&reset, 0, sizeof(reset));
     reset.nseeds = sc.nseeds;
-    reset.outstanding.v = sc.nseeds;
-    reset.done.v = sc.nseeds == 0;
     CK(cudaMemcpyAsync(d_sched.ptr, &reset, sizeof(reset), cudaMemcpyHostToDevice, stream));
     CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
+    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream);
+    ++stats.kernel_launches;
     CK(cudaStreamSynchronize(stream));
   }
   unsigned int err_host[4] = {0, 0, 0, 0};

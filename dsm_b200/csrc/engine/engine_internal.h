@@ -68,7 +68,7 @@ struct Engine {
   int label_quirk = 0;
   int sort_results = 1;
   uint64_t result_cap = 1 << 20;
-  uint32_t job_cap = 1 << 20;
+  uint32_t job_ring = 1 << 19;  // job slots of the matcher's donation ring
   uint64_t list_limit_bytes = 8ull << 30;  // beyond this a batch returns counts only
 
   // graph
@@ -88,9 +88,8 @@ struct Engine {
 
   // batch scratch
   DevBuf d_upd, d_bkey, d_bidx, d_binfo, d_gflag, d_vtp, d_dkey, d_dhead, d_dsel, d_seeds, d_sched, d_jobs,
-      d_job_ready, d_out_seg, d_out_tup, d_segcnt, d_misc;
+      d_job_seq, d_out_seg, d_out_tup, d_segcnt, d_misc;
   HostBuf h_stage, h_sched, h_segcnt, h_vtp, h_out_seg, h_out_tup;
-  uint32_t epoch = 0;
 
   // results
   std::map<uint64_t, std::unique_ptr<BatchResult>> results;

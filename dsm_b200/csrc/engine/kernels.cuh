@@ -66,11 +66,10 @@ struct MatchArgs {
   const OrderRec *orders;
   const uint4 *seeds;
   Sched *sc;
-  JobRec *jobs;
-  uint32_t *job_ready;
-  uint32_t job_cap;    // donors stop reserving at this many slots
-  uint32_t job_slots;  // allocated slots: job_cap + room for racing reservations
-  uint32_t epoch;
+  JobRec *jobs;                  // ring of job records
+  unsigned long long *job_seq;   // per slot: p = free for position p, t + 1 = job
+                                 // for ticket t, t | kSeqDone = no more work
+  uint32_t job_ring;             // slots, a power of two
   uint32_t *out_seg;
   uint32_t *out_tup;
   uint32_t W;
@@ -80,7 +79,10 @@ struct MatchArgs {
   int donate;
   long long timeout_cycles;
 };
-void launch_sched_init(Sched *sc, unsigned long long seed_cap, cudaStream_t s);
+// Arms a matcher launch: outstanding = seeds, every ring slot free for its
+// first position.
+void launch_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long long *job_seq, uint32_t job_ring,
+                       cudaStream_t s);
 void launch_match(const MatchArgs &a, int blocks, cudaStream_t s);
 int match_max_blocks_per_sm();
 

@@ -31,9 +31,10 @@ __device__ __forceinline__ T ld_volatile(const T &x) {
   return *(const volatile T *)&x;
 }
 
-constexpr uint32_t kSlotDone = 0x80000000u;
+constexpr unsigned long long kSeqDone = 1ull << 63;
 
-// Lane 0 only.  Returns 1 (seed `slot`), 2 (job `slot`) or 0 (no more work).
+// Lane 0 only.  Returns 1 (seed `slot`), 2 (job of ticket `slot`; the caller
+// releases the ring slot after reading it) or 0 (no more work).
 __device__ uint32_t acquire(const MatchArgs &P, unsigned long long &slot, bool &seeds_done) {
   Sched *sc = P.sc;
   if (!seeds_done) {
@@ -53,18 +54,17 @@ __device__ uint32_t acquire(const MatchArgs &P, unsigned long long &slot, bool &
   long long t0 = clock64();
   unsigned long long last_prog = ld_volatile(sc->progress.v);
   unsigned ns = 32;
+  const unsigned long long *seq = P.job_seq + (t & (P.job_ring - 1));
   for (uint32_t it = 0;; ++it) {
-    if (t < P.job_slots) {
-      uint32_t r = ld_volatile(P.job_ready[t]);
-      if (r == P.epoch) {
-        __threadfence();
-        slot = t;
-        atomicAdd(&sc->steals, 1ull);
-        return 2;
-      }
-      if (r == (P.epoch | kSlotDone)) return 0;
+    unsigned long long r = ld_volatile(*seq);
+    if (r == t + 1) {
+      __threadfence();
+      slot = t;
+      atomicAdd(&sc->steals, 1ull);
+      return 2;
     }
-    if ((it & 7) == 7 || t >= P.job_slots) {
+    if (r == (t | kSeqDone)) return 0;
+    if ((it & 7) == 7) {
       if (ld_volatile(sc->done.v) || ld_volatile(sc->error)) return 0;
       unsigned long long pr = ld_volatile(sc->progress.v);
       if (pr != last_prog) {
@@ -87,7 +87,10 @@ __device__ void finish_task(const MatchArgs &P) {
   if (lane == 0) before = atomicAdd(&P.sc->outstanding.v, ~0ull);
   before = __shfl_sync(kFull, before, 0);
   if (before != 1) return;
-  // last task of the launch: release every warp still waiting on a ticket
+  // Last task of the launch: release every warp still waiting on a ticket.
+  // Every position below push_cnt has been consumed (nothing is outstanding),
+  // so the slot of each waiting ticket t is free and holds t; at most one
+  // ticket per warp waits, far fewer than the ring's slots.
   unsigned long long lo = 0, hi = 0;
   if (lane == 0) {
     atomicExch(&P.sc->done.v, 1ull);
@@ -96,8 +99,9 @@ __device__ void finish_task(const MatchArgs &P) {
     lo = ld_volatile(P.sc->push_cnt.v);
   }
   lo = __shfl_sync(kFull, lo, 0);
-  hi = min(__shfl_sync(kFull, hi, 0), (unsigned long long)P.job_slots);
-  for (unsigned long long s = lo + lane; s < hi; s += 32) atomicExch(&P.job_ready[s], P.epoch | kSlotDone);
+  hi = __shfl_sync(kFull, hi, 0);
+  for (unsigned long long t = lo + lane; t < hi; t += 32)
+    atomicExch(&P.job_seq[t & (P.job_ring - 1)], t | kSeqDone);
 }
 
 __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t depth, uint32_t lo,
@@ -278,13 +282,26 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
             }
             unsigned long long s0 = 0;
             uint32_t okr = 0;
+            const unsigned long long rmask = P.job_ring - 1;
             if (lane == 0) {
-              if (ld_volatile(P.sc->push_cnt.v) + k <= P.job_cap) {
-                atomicAdd(&P.sc->outstanding.v, (unsigned long long)k);
-                s0 = atomicAdd(&P.sc->push_cnt.v, (unsigned long long)k);
-                okr = 1;
-                atomicAdd(&P.sc->donations, (unsigned long long)k);
-              }
+              // k <= waiting warps, so positions stay within one warp's worth
+              // of reservations per donor of pop_cnt: the slot of position p
+              // was last used by position p - ring, consumed long ago; wait
+              // (bounded) until its consumer has released it
+              atomicAdd(&P.sc->outstanding.v, (unsigned long long)k);
+              s0 = atomicAdd(&P.sc->push_cnt.v, (unsigned long long)k);
+              atomicAdd(&P.sc->donations, (unsigned long long)k);
+              okr = 1;
+              long long tw = clock64();
+              for (uint32_t r = 0; r < k && okr; ++r)
+                while (ld_volatile(P.job_seq[(s0 + r) & rmask]) != s0 + r) {
+                  if (clock64() - tw > P.timeout_cycles) {
+                    atomicOr(&P.sc->error, kErrTimeout);
+                    okr = 0;
+                    break;
+                  }
+                  __nanosleep(64);
+                }
             }
             okr = __shfl_sync(kFull, okr, 0);
             s0 = __shfl_sync(kFull, s0, 0);
@@ -315,12 +332,12 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
                   uint32_t fi = lane - 8;
                   word = fi < p ? fsrc : (fi == p && pm ? cw : 0u);
                 }
-                uint32_t *rec = reinterpret_cast<uint32_t *>(P.jobs + s0 + r);
+                uint32_t *rec = reinterpret_cast<uint32_t *>(P.jobs + ((s0 + r) & rmask));
                 __stcg(rec + lane, word);
               }
               __threadfence();
               __syncwarp();
-              if (lane < k) atomicExch(&P.job_ready[s0 + lane], P.epoch);
+              if (lane < k) atomicExch(&P.job_seq[(s0 + lane) & rmask], s0 + lane + 1);
               if (lane == p) {
                 if (pm) lv_mask &= ~dmask;
                 else lv_end = rmid;
@@ -350,14 +367,19 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
   flush();
 }
 
-__global__ void k_sched_init(Sched *sc, unsigned long long seed_cap) {
-  unsigned long long n = sc->nseeds;
-  if (n > seed_cap) {
-    sc->nseeds = n = seed_cap;
-    atomicOr(&sc->error, kErrSeeds);
+__global__ void k_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long long *job_seq,
+                             uint32_t job_ring) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint32_t s = i; s < job_ring; s += gridDim.x * blockDim.x) job_seq[s] = s;
+  if (i == 0) {
+    unsigned long long n = sc->nseeds;
+    if (n > seed_cap) {
+      sc->nseeds = n = seed_cap;
+      atomicOr(&sc->error, kErrSeeds);
+    }
+    sc->outstanding.v = n;
+    sc->done.v = (n == 0) ? 1ull : 0ull;
   }
-  sc->outstanding.v = n;
-  sc->done.v = (n == 0) ? 1ull : 0ull;
 }
 
 __global__ void __launch_bounds__(256) k_match(MatchArgs P) {
@@ -378,8 +400,13 @@ __global__ void __launch_bounds__(256) k_match(MatchArgs P) {
       depth = 2;
       fval = lane == 0 ? s.z : (lane == 1 ? s.w : 0u);
     } else {
-      const uint32_t *rec = reinterpret_cast<const uint32_t *>(P.jobs + slot);
+      const uint32_t *rec = reinterpret_cast<const uint32_t *>(P.jobs + (slot & (P.job_ring - 1)));
       uint32_t word = __ldcg(rec + lane);
+      __syncwarp();
+      if (lane == 0) {  // the slot is free for position slot + ring
+        __threadfence();
+        atomicExch(&P.job_seq[slot & (P.job_ring - 1)], slot + P.job_ring);
+      }
       upd = __shfl_sync(kFull, word, 0);
       qo = __shfl_sync(kFull, word, 1);
       depth = __shfl_sync(kFull, word, 2);
@@ -394,8 +421,9 @@ __global__ void __launch_bounds__(256) k_match(MatchArgs P) {
 
 }  // namespace
 
-void launch_sched_init(Sched *sc, unsigned long long seed_cap, cudaStream_t s) {
-  k_sched_init<<<1, 1, 0, s>>>(sc, seed_cap);
+void launch_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long long *job_seq, uint32_t job_ring,
+                       cudaStream_t s) {
+  k_sched_init<<<(job_ring + 255) / 256, 256, 0, s>>>(sc, seed_cap, job_seq, job_ring);
 }
 
 void launch_match(const MatchArgs &a, int blocks, cudaStream_t s) {
