@@ -110,6 +110,8 @@ def run_ours(args, rank, world):
     gen_s = time.time() - t0
     batches = list(w.batches())
     queries = w.queries
+    print(f"[bench] workload generated in {gen_s:.1f} s: {w.nv} vertices, {len(w.edges)} edges, "
+          f"queries {[q.labels.tolist() for q in queries]}", file=sys.stderr, flush=True)
 
     def new_engine(qs):
         e = d.Engine(dev)
@@ -121,6 +123,7 @@ def run_ours(args, rank, world):
         engines = [new_engine(queries)]
     else:
         engines = [new_engine([q]) for q in queries]
+    print(f"[bench] {len(engines)} engine(s) loaded", file=sys.stderr, flush=True)
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MiB > L2
 
     def step(b):

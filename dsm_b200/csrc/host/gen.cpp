@@ -271,7 +271,7 @@ bool sample_query(const Adj &g, const std::vector<uint32_t> &labels, const std::
                   Query &q) {
   const uint32_t nv = (uint32_t)labels.size();
   const bool selective = max_mean > 0 && !probe.empty();
-  constexpr int kPerTier = 12;
+  constexpr int kPerTier = 64;
   const uint32_t nlabels = (uint32_t)label_rank.size();
   const uint32_t tiers = selective ? std::max<uint32_t>(1, nlabels > 3 ? nlabels - 3 : 1) : 1;
   double best_total = 1e300;
@@ -279,8 +279,11 @@ bool sample_query(const Adj &g, const std::vector<uint32_t> &labels, const std::
   for (uint32_t tier = 0; tier < tiers; ++tier) {
     auto allowed = [&](uint32_t v) { return label_rank[labels[v]] >= tier; };
     int scored = 0;
-    for (int attempt = 0; attempt < 4000 && scored < kPerTier; ++attempt) {
-      uint32_t start = (uint32_t)r.below(nv);
+    for (int attempt = 0; attempt < 20000 && scored < kPerTier; ++attempt) {
+      // dense shapes need the dense part of the graph: those walks start at
+      // the end of a uniformly drawn edge (degree-biased), the others at a
+      // uniformly drawn vertex
+      uint32_t start = extra * 2 > nq ? g.nbr[r.below(g.nbr.size())] : (uint32_t)r.below(nv);
       if (g.deg(start) == 0 || !allowed(start)) continue;
       std::vector<uint32_t> vs{start};
       std::vector<std::pair<uint32_t, uint32_t>> tree;
