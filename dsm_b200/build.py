@@ -30,6 +30,7 @@ LIB_SOURCES = [
     
     "engine/engine.cu",
     "engine/abi.cu",
+    "engine/noalloc.cu",
     "host/gen.cpp",
     "host/textio.cpp",
     "host/query_plan.cpp",

@@ -141,6 +141,41 @@ typedef struct dsm_result_view {
 int dsm_batch_results(dsm_engine *e, uint64_t batch_id, dsm_result_view *view);
 int dsm_batch_release(dsm_engine *e, uint64_t batch_id);
 
+/* ---- counting without allocating ------------------------------------- */
+/* No counterpart in the reference: an entry point for callers that must not
+ * allocate device memory while they run -- code living inside a framework
+ * that owns the device allocator and forbids side allocations, or a thread
+ * that must not call cudaMalloc / cudaFree because those calls synchronise
+ * the whole device.  It needs no engine: the caller passes a fixed graph,
+ * the updates and the output, all in device memory, and the matcher's scratch
+ * (scheduler counters, donation ring, seed table, query descriptor) lives in
+ * one static device array of about 12.5 MB that every GPU loading this
+ * library holds until the process exits.
+ *
+ * For each update i, d_counts[i] = the number of embeddings of the query that
+ * map some query edge onto {src, dst} in the graph with that edge present
+ * (the count an insert of the edge would report; the op and label fields are
+ * not read).  src must differ from dst.
+ *   graph: d_adj holds 2 words per vertex, {start of the vertex's run in
+ *          16-byte units, degree}; the run d_arena[4*start .. 4*start+degree)
+ *          lists its neighbours sorted ascending, without duplicates;
+ *          d_labels[v] < 2^31.
+ *   query: host CSR as for dsm_query_register, at most 8 vertices.
+ *   limits: n <= 4096 updates (DSM_ERR_LIMIT beyond).
+ *   stream: a cudaStream_t (NULL = the default stream); the call returns once
+ *           the counts are written.
+ * The first call on a device looks the static array's device address up
+ * (cudaGetSymbolAddress, with `device` made current) and should come before
+ * any stream capture.  Every call reuses the same array and clears what must
+ * start at zero; calls whose work overlaps on the GPU race on it.  Nothing is
+ * allocated: no cudaMalloc, no cudaFree. */
+int dsm_count_edge_embeddings_noalloc(int device, uint32_t nv, const uint32_t *d_adj,
+                                      const uint32_t *d_arena, const uint32_t *d_labels,
+                                      const uint32_t *q_offsets, const uint32_t *q_nbrs,
+                                      const uint32_t *q_labels, uint32_t nq,
+                                      const dsm_update *d_updates, uint32_t n, uint64_t *d_counts,
+                                      void *stream);
+
 /* ---- statistics ------------------------------------------------------- */
 typedef struct dsm_stats {
   uint64_t batches;
