@@ -27,6 +27,7 @@ CXX_FLAGS = COMMON
 LIB_SOURCES = [
     "engine/kernels.cu",
     "engine/match.cu",
+    "engine/filter.cu",
     
     "engine/engine.cu",
     "engine/abi.cu",

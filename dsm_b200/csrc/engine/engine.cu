@@ -19,6 +19,7 @@
 #include "../host/dsm_host.h"
 #include "../host/query_plan.h"
 #include "engine_internal.h"
+#include "filter.cuh"
 #include "kernels.cuh"
 
 namespace dsm {
@@ -118,6 +119,7 @@ std::vector<DevBuf *> Engine::all_dev_bufs() {
                              &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc};
   for (auto &q : slots) v.push_back(&q.bitmap);
   for (auto &q : slots) v.push_back(&q.filter_scratch);
+  for (auto &q : slots) v.push_back(&q.filter_plan);
   return v;
 }
 
@@ -641,6 +643,13 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   stats.last_batch_ms = ms_total;
   stats.last_match_ms = ms_match;
   stats.last_update_ms = ms_upd;
+  stats.last_filter_ms = 0;
+  if (filter_timed) {
+    float fm = 0;
+    cudaEventElapsedTime(&fm, ev_pool[5], ev_pool[6]);
+    stats.last_filter_ms = fm;
+    filter_timed = false;
+  }
   R.device_ms = ms_total;
   R.match_ms = ms_match;
   R.alg_bytes = sc.alg_bytes;
@@ -648,11 +657,122 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   return DSM_OK;
 }
 
-int Engine::run_filters() { return DSM_OK; }
+// Uploads the filter's descriptor and op list of query `id` and sizes its
+// per-vertex buffers (once per registration / graph load).
+int Engine::prepare_filter(uint32_t id) {
+  Slot &s = slots[id];
+  if (!s.filter_dirty && s.filter_scratch.ptr && s.bitmap.ptr) return DSM_OK;
+  const QueryPlan &p = s.plan;
+  QFilterDesc desc;
+  std::memset(&desc, 0, sizeof(desc));
+  desc.nq = p.nq;
+  desc.nlabels = p.nlabels;
+  for (uint32_t u = 0; u < p.nq; ++u) {
+    desc.label_us[p.labels[u]] |= 1u << u;
+    desc.qdeg[u] = p.degree[u];
+    desc.pos_of_u[u] = p.enc_pos_of_u[u];
+    for (uint32_t l = 0; l < 32; ++l) desc.nlc[u][l] = (uint8_t)std::min<uint32_t>(p.nlc[(size_t)u * 32 + l], 255);
+  }
+  std::vector<DevFilterOp> ops(p.ops.size());
+  for (size_t k = 0; k < p.ops.size(); ++k) {
+    const FilterOp &o = p.ops[k];
+    DevFilterOp &d = ops[k];
+    std::memset(&d, 0, sizeof(d));
+    d.kind = o.kind;
+    d.core_u = o.core_u;
+    d.pos = o.pos;
+    d.nleaf = o.nleaf;
+    for (int i = 0; i < 16; ++i) d.leaf_u[i] = o.leaf_u[i];
+    d.lp = o.left_pos;
+    d.rp = o.right_pos;
+    d.lcp = o.left_core_pos;
+    d.rcp = o.right_core_pos;
+    d.comb_type = o.comb_type;
+    d.nsmall = o.nsmall;
+    for (int i = 0; i < 32; ++i) d.small_core_pos[i] = o.small_core_pos[i];
+    for (int i = 0; i < 16; ++i) {
+      d.leaf_src_count[i] = o.leaf_src_count[i];
+      for (int j = 0; j < 32; ++j) d.leaf_src[i][j] = (uint16_t)o.leaf_src[i][j];
+    }
+  }
+  const size_t plan_bytes = sizeof(QFilterDesc) + ops.size() * sizeof(DevFilterOp);
+  const uint32_t col_len = (nv + 31) / 32;
+  const size_t words = std::max<uint32_t>(p.enc_words, 1);
+  int rc;
+  if ((rc = dalloc(s.filter_plan, plan_bytes)) || (rc = dalloc(s.filter_scratch, (size_t)nv * (8 + 4 * words))) ||
+      (rc = dalloc(s.bitmap, (size_t)p.nq * col_len * 4)))
+    return rc;
+  CK(cudaMemcpyAsync(s.filter_plan.ptr, &desc, sizeof(desc), cudaMemcpyHostToDevice, stream));
+  if (!ops.empty())
+    CK(cudaMemcpyAsync((char *)s.filter_plan.ptr + sizeof(QFilterDesc), ops.data(), ops.size() * sizeof(DevFilterOp),
+                       cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));  // `desc` and `ops` are stack / vector memory
+  s.filter_nops = (uint32_t)ops.size();
+  s.filter_dirty = false;
+  return DSM_OK;
+}
 
-int Engine::query_filter(uint32_t, uint32_t *, uint32_t *) {
+int Engine::launch_filter(uint32_t id, int mode) {
+  Slot &s = slots[id];
+  FilterDevice f;
+  f.desc = (const QFilterDesc *)s.filter_plan.ptr;
+  f.ops = (const DevFilterOp *)((const char *)s.filter_plan.ptr + sizeof(QFilterDesc));
+  f.nops = s.filter_nops;
+  f.vcand = (uint32_t *)s.filter_scratch.ptr;
+  f.valid = f.vcand + nv;
+  f.enc = f.valid + nv;
+  f.words = std::max<uint32_t>(s.plan.enc_words, 1);
+  f.col_len = (nv + 31) / 32;
+  f.bitmap = (uint32_t *)s.bitmap.ptr;
+  launch_query_filter(dev_graph(), f, mode, num_sms, stream);
+  stats.kernel_launches += 2 + (mode >= 2 ? f.nops : 0);
+  return DSM_OK;
+}
+
+// Candidate filters of every live query on the batch's union graph (sound
+// for every state the batch passes through); the matcher and the seeds then
+// test each candidate against its query vertex's bitmap.
+int Engine::run_filters() {
+  bool changed = false;
+  for (uint32_t id : live_ids) {
+    QDev &q = qd_host[id];
+    const uint32_t *want = nullptr;
+    if (filter_mode > 0) {
+      if (int rc = prepare_filter(id)) return rc;
+      want = (const uint32_t *)slots[id].bitmap.ptr;
+    }
+    if (q.bitmap != want) {
+      q.bitmap = want;
+      changed = true;
+    }
+  }
+  if (changed)
+    if (int rc = upload_qd()) return rc;
+  if (filter_mode == 0) return DSM_OK;
+  cudaEvent_t f0 = ev_pool[5], f1 = ev_pool[6];
+  CK(cudaEventRecord(f0, stream));
+  for (uint32_t id : live_ids)
+    if (int rc = launch_filter(id, filter_mode)) return rc;
+  CK(cudaEventRecord(f1, stream));
+  filter_timed = true;
+  return DSM_OK;
+}
+
+int Engine::query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us) {
   std::lock_guard<std::mutex> lk(mu);
-  return fail(DSM_ERR_STATE, "candidate filter not available");
+  if (!graph_loaded) return fail(DSM_ERR_STATE, "no graph loaded");
+  if (qid >= slots.size() || !slots[qid].live) return fail(DSM_ERR_NOT_FOUND, "no such query");
+  CK(cudaSetDevice(device));
+  if (int rc = prepare_filter(qid)) return rc;
+  if (int rc = launch_filter(qid, 2)) return rc;
+  CK(cudaGetLastError());
+  const Slot &s = slots[qid];
+  if (bitmaps)
+    CK(cudaMemcpyAsync(bitmaps, s.bitmap.ptr, (size_t)s.plan.nq * ((nv + 31) / 32) * 4, cudaMemcpyDeviceToHost,
+                       stream));
+  if (v_cand_us) CK(cudaMemcpyAsync(v_cand_us, s.filter_scratch.ptr, (size_t)nv * 4, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  return DSM_OK;
 }
 
 int Engine::view(uint64_t id, dsm_result_view *v) {

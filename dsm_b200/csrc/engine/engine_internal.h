@@ -31,8 +31,10 @@ struct Slot {
   bool live = false;
   QueryPlan plan;
   DevBuf bitmap;          // nq x col_len candidate bitmaps
-  DevBuf filter_scratch;  // encodings, candidate lists
-  bool filter_dirty = true;
+  DevBuf filter_scratch;  // vcand, valid, encodings (per data vertex)
+  DevBuf filter_plan;     // QFilterDesc + op list
+  uint32_t filter_nops = 0;
+  bool filter_dirty = true;  // plan or sizes must be (re)uploaded
 };
 
 struct BatchResult {
@@ -67,6 +69,7 @@ struct Engine {
   int64_t timeout_ms = 5000;
   int label_quirk = 0;
   int sort_results = 1;
+  bool filter_timed = false;  // the filter events of this batch were recorded
   uint64_t result_cap = 1 << 20;
   uint32_t job_ring = 1 << 19;  // job slots of the matcher's donation ring
   uint64_t list_limit_bytes = 8ull << 30;  // beyond this a batch returns counts only
@@ -114,6 +117,8 @@ struct Engine {
   int sync_queries();
   int upload_qd();
   int run_filters();
+  int prepare_filter(uint32_t id);
+  int launch_filter(uint32_t id, int mode);
   int query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);
 
   int submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id);
