@@ -116,6 +116,7 @@ def run_ours(args, rank, world):
     def new_engine(qs):
         e = d.Engine(dev)
         e.set_option(d.OPT_LIST, args.list)
+        e.set_option(d.OPT_FILTER, args.filter)
         e.load_graph_edges(w.nv, w.labels, w.edges)
         return e, [e.register(q) for q in qs]
 
@@ -147,7 +148,7 @@ def run_ours(args, rank, world):
             d2h += r.tuples.nbytes + r.counts.nbytes + r.signs.nbytes
             if args.verbose:
                 print(f"  engine {qids}: dev {s1['last_batch_ms']:.2f} ms match {s1['last_match_ms']:.2f} ms "
-                      f"upd {s1['last_update_ms']:.2f} ms wall {(time.perf_counter() - tw) * 1e3:.1f} ms "
+                      f"upd {s1['last_update_ms']:.2f} ms filter {s1['last_filter_ms']:.2f} ms wall {(time.perf_counter() - tw) * 1e3:.1f} ms "
                       f"matches {int(r.counts.sum())} per-query {r.counts.sum(axis=1).tolist()} "
                       f"seeds {s1['seeds'] - s0['seeds']} donations {s1['donations'] - s0['donations']} "
                       f"listed {r.listed}", file=sys.stderr, flush=True)
@@ -205,7 +206,7 @@ def run_ours(args, rank, world):
         "data": "synthetic (seeded Chung-Lu graph, random-walk queries, generated update stream)",
         "config": {"workload": f"config2: Chung-Lu gamma=2.1, |V|=2^{20 + args.scale}, |E|=2^{24 + args.scale}, "
                                "16 Zipf(1.2) labels, three 8-vertex queries, batches of 4096 (50/50)",
-                   "form": args.form, "listing": bool(args.list), "parallelism": f"replicas x{world}",
+                   "form": args.form, "listing": bool(args.list), "filter": args.filter, "parallelism": f"replicas x{world}",
                    "l2": "256 MiB buffer written between timed batches"},
         "updates_per_sec": upd / (dev_ms / 1e3) if dev_ms > 0 else 0.0,
         "matches": matches,
@@ -281,6 +282,7 @@ def main():
     # at full size: the default measures exact counts (listing is covered by
     # the parity tests); --list 1 lists and sorts them as well
     ap.add_argument("--list", type=int, default=0)
+    ap.add_argument("--filter", type=int, default=0, help="candidate filter: 0 none, 1 LDF+NLF, 2 cluster encoding")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--scale", type=int, default=0, help="log2 shrink of the graph (0 = config size)")
     ap.add_argument("--cpu-sample", type=int, default=256)

@@ -13,16 +13,36 @@ constexpr uint32_t kTouchBit = 0x80000000u;  // label word bit: endpoint of an u
 constexpr uint32_t kLabelMask = 0x7FFFFFFFu;
 constexpr uint32_t kNoView = 0xFFFFFFFFu;     // view time of a no-op update
 
-// Data graph in HBM.  Each vertex owns a sorted run of neighbour ids in one
-// arena; runs start on 16-byte boundaries and carry slack so that inserts
-// merge in place.  adj[v] = {start in 16-byte units, degree}: one 8-byte load
-// gives both.
+// Adjacency entries are label-major: entry = slot(label) << 27 | id, where
+// slot(label) = min(label, 31), so a run sorted by entry value lists its
+// neighbours by label, then id, and the neighbours with one label form one
+// contiguous range.  Slot 31 is shared by every label >= 31; a query vertex
+// with label 31 checks the exact label of what it takes from that slot.
+constexpr uint32_t kIdBits = 27;
+constexpr uint32_t kIdMask = (1u << kIdBits) - 1;
+constexpr uint32_t kMaxVertices = 1u << kIdBits;
+constexpr uint32_t kSlots = 32;
+__host__ __device__ __forceinline__ uint32_t label_slot(uint32_t label) { return label < 31 ? label : 31; }
+__host__ __device__ __forceinline__ uint32_t pack_entry(uint32_t label, uint32_t v) {
+  return (label_slot(label) << kIdBits) | v;
+}
+
+// Data graph in HBM.  Each vertex owns a sorted run of entries in one arena;
+// runs start on 16-byte boundaries and carry slack so that inserts merge in
+// place.  adj[v] = {start in 16-byte units, degree}: one 8-byte load gives
+// both.  loff[v * (nlt + 1) + s] = index in v's run of its first entry with
+// slot >= s (s = 0..nlt; nlt = number of slots in use), so the neighbours of
+// v with slot s are [loff[s], loff[s + 1]): one 8-byte read per lookup.
+// loff == nullptr marks plain runs (neighbour ids sorted ascending), the
+// layout callers of the allocation-free entry point pass.
 struct DevGraph {
   uint32_t nv;
   uint32_t *lab;       // [nv] label | kTouchBit
   uint2 *adj;          // [nv] {off16, deg}
   uint32_t *cap;       // [nv] capacity in entries (multiple of 4)
-  uint32_t *arena;     // neighbour ids
+  uint32_t *arena;     // entries
+  uint32_t *loff;      // [nv * (nlt + 1)] slot offsets, or null for plain runs
+  uint32_t nlt;
   uint64_t arena_words;
   unsigned long long *arena_top;  // next free 16-byte unit
 };

@@ -113,7 +113,7 @@ Engine::~Engine() {
 }
 
 std::vector<DevBuf *> Engine::all_dev_bufs() {
-  std::vector<DevBuf *> v = {&d_lab, &d_adj, &d_cap, &d_arena, &d_arena_top, &d_qd, &d_orders,
+  std::vector<DevBuf *> v = {&d_lab, &d_adj, &d_cap, &d_arena, &d_arena_top, &d_loff, &d_qd, &d_orders,
                              &d_pair_off, &d_pair_ent, &d_upd, &d_bkey, &d_bidx, &d_binfo, &d_gflag,
                              &d_vtp, &d_dkey, &d_dhead, &d_dsel, &d_seeds, &d_sched, &d_jobs,
                              &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc};
@@ -159,8 +159,13 @@ int Engine::load_graph(uint32_t nv_, const uint32_t *labels, std::vector<uint64_
   std::lock_guard<std::mutex> lk(mu);
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
-  for (uint32_t v = 0; v < nv_; ++v)
+  if (nv_ > kMaxVertices) return fail(DSM_ERR_LIMIT, "more than 2^27 vertices");
+  uint32_t max_label = 0;
+  for (uint32_t v = 0; v < nv_; ++v) {
     if (labels[v] & kTouchBit) return fail(DSM_ERR_LIMIT, "vertex label >= 2^31");
+    max_label = std::max(max_label, labels[v]);
+  }
+  const uint32_t nlt_ = nv_ ? label_slot(max_label) + 1 : 1;
   // canonical, deduplicated undirected edges
   std::sort(keys.begin(), keys.end());
   keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
@@ -186,24 +191,35 @@ int Engine::load_graph(uint32_t nv_, const uint32_t *labels, std::vector<uint64_
   HostBuf stage;
   if (int rc = halloc(stage, used_words * 4)) return rc;
   uint32_t *h_arena = (uint32_t *)stage.ptr;
+  // label-major runs: entries sorted by (label slot, id), and each vertex's
+  // slot offsets
   std::vector<uint32_t> fill(nv_, 0);
   for (uint64_t k : keys) {
     uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
-    h_arena[(uint64_t)adj[a].x * 4 + fill[a]++] = b;
-    h_arena[(uint64_t)adj[b].x * 4 + fill[b]++] = a;
+    h_arena[(uint64_t)adj[a].x * 4 + fill[a]++] = pack_entry(labels[b], b);
+    h_arena[(uint64_t)adj[b].x * 4 + fill[b]++] = pack_entry(labels[a], a);
   }
+  const size_t stride = nlt_ + 1;
+  std::vector<uint32_t> loff((size_t)nv_ * stride);
   for (uint32_t v = 0; v < nv_; ++v) {
     uint32_t *run = h_arena + (uint64_t)adj[v].x * 4;
     std::sort(run, run + deg[v]);
     for (uint32_t i = deg[v]; i < cap[v]; ++i) run[i] = 0xFFFFFFFFu;
     adj[v].y = deg[v];
+    uint32_t *t = loff.data() + (size_t)v * stride;
+    for (uint32_t sl = 0, i = 0; sl <= nlt_; ++sl) {
+      while (i < deg[v] && (run[i] >> kIdBits) < sl) ++i;
+      t[sl] = sl == nlt_ ? deg[v] : i;
+    }
   }
   int rc;
   if ((rc = dalloc(d_lab, (size_t)nv_ * 4)) || (rc = dalloc(d_adj, (size_t)nv_ * 8)) ||
-      (rc = dalloc(d_cap, (size_t)nv_ * 4)) || (rc = dalloc(d_arena, arena_words * 4))) {
+      (rc = dalloc(d_cap, (size_t)nv_ * 4)) || (rc = dalloc(d_loff, loff.size() * 4)) ||
+      (rc = dalloc(d_arena, arena_words * 4))) {
     cudaFreeHost(stage.ptr);
     return rc;
   }
+  CK(cudaMemcpyAsync(d_loff.ptr, loff.data(), loff.size() * 4, cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d_lab.ptr, labels, (size_t)nv_ * 4, cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d_adj.ptr, adj.data(), (size_t)nv_ * 8, cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d_cap.ptr, cap.data(), (size_t)nv_ * 4, cudaMemcpyHostToDevice, stream));
@@ -213,6 +229,7 @@ int Engine::load_graph(uint32_t nv_, const uint32_t *labels, std::vector<uint64_
   CK(cudaStreamSynchronize(stream));
   cudaFreeHost(stage.ptr);
   nv = nv_;
+  nlt = nlt_;
   this->arena_words = arena_words;
   arena_used16 = off16;
   graph_entries = 2 * keys.size();
@@ -229,6 +246,8 @@ DevGraph Engine::dev_graph() {
   g.adj = (uint2 *)d_adj.ptr;
   g.cap = (uint32_t *)d_cap.ptr;
   g.arena = (uint32_t *)d_arena.ptr;
+  g.loff = (uint32_t *)d_loff.ptr;
+  g.nlt = nlt;
   g.arena_words = arena_words;
   g.arena_top = (unsigned long long *)d_arena_top.ptr;
   return g;
@@ -253,11 +272,17 @@ int Engine::export_graph(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entrie
     offsets[nv] = (uint32_t)k;
   }
   if (nbrs) {
+    // one copy of the arena's used part, then per run: ids, ascending
+    unsigned long long top16 = 0;
+    CK(cudaMemcpy(&top16, d_arena_top.ptr, 8, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> arena(top16 * 4);
+    if (!arena.empty())
+      CK(cudaMemcpy(arena.data(), d_arena.ptr, arena.size() * 4, cudaMemcpyDeviceToHost));
     uint64_t k = 0;
     for (uint32_t v = 0; v < nv; ++v) {
-      if (adj[v].y)
-        CK(cudaMemcpy(nbrs + k, (uint32_t *)d_arena.ptr + (uint64_t)adj[v].x * 4, (size_t)adj[v].y * 4,
-                      cudaMemcpyDeviceToHost));
+      const uint32_t *run = arena.data() + (uint64_t)adj[v].x * 4;
+      for (uint32_t i = 0; i < adj[v].y; ++i) nbrs[k + i] = run[i] & kIdMask;
+      std::sort(nbrs + k, nbrs + k + adj[v].y);
       k += adj[v].y;
     }
   }
@@ -403,10 +428,10 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   const uint32_t m = (uint32_t)und.size();
   std::vector<uint64_t> dir;
   dir.reserve(2 * (size_t)m);
-  for (auto &e : und) {
+  for (auto &e : und) {  // x << 32 | entry of y, so each group is in run order
     uint32_t a = (uint32_t)(e.first >> 32), b = (uint32_t)e.first;
-    dir.push_back(((uint64_t)a << 32) | b);
-    dir.push_back(((uint64_t)b << 32) | a);
+    dir.push_back(((uint64_t)a << 32) | entry_of(b));
+    dir.push_back(((uint64_t)b << 32) | entry_of(a));
   }
   std::sort(dir.begin(), dir.end());
   std::vector<uint32_t> dhead;

@@ -78,8 +78,9 @@ struct Engine {
   bool graph_loaded = false;
   uint32_t nv = 0;
   uint64_t arena_words = 0, arena_used16 = 0, graph_entries = 0;
+  uint32_t nlt = 0;  // label slots in use (slot offsets per vertex: nlt + 1)
   std::vector<uint32_t> label_host;
-  DevBuf d_lab, d_adj, d_cap, d_arena, d_arena_top;
+  DevBuf d_lab, d_adj, d_cap, d_arena, d_arena_top, d_loff;
 
   // queries
   std::vector<Slot> slots;
@@ -109,6 +110,7 @@ struct Engine {
   std::vector<DevBuf *> all_dev_bufs();
 
   int load_graph(uint32_t nv, const uint32_t *labels, std::vector<uint64_t> &keys);
+  uint32_t entry_of(uint32_t v) const { return pack_entry(label_host[v], v); }
   DevGraph dev_graph();
   int export_graph(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries);
 

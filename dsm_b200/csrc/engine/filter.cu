@@ -2,7 +2,8 @@
 // oneRoundFilterBidirectionKernel 394-613, encode/merge/combine 615-1177,
 // compact 1692-1749), run per query on the batch's union graph.
 //
-// Layout per query: vcand[v] (bit u: v passes LDF+NLF for u, the
+// The graph's runs are label-major (entries carry the label slot above the
+// id).  Layout per query: vcand[v] (bit u: v passes LDF+NLF for u, the
 // reference's d_v_candidate_us_), valid[v] (bit u: v is still a candidate
 // of u; merges and combines clear bits, as the reference overwrites entries
 // of its per-u candidate lists), enc[v * words + pos / 32] (cluster
@@ -53,7 +54,7 @@ __global__ void k_ldf_nlf(DevGraph g, const QFilterDesc *D, uint32_t *vcand, uin
       __syncwarp();
       const uint32_t *run = adj_list(g, av);
       for (uint32_t i = lane; i < av.y; i += 32) {
-        uint32_t l = g.lab[run[i]] & kLabelMask;
+        uint32_t l = g.lab[run[i] & kIdMask] & kLabelMask;
         if (l < nl) atomicAdd(&cnt[wib][l], 1u);
       }
       __syncwarp();
@@ -108,7 +109,7 @@ __global__ void k_filter_op(DevGraph g, const DevFilterOp *ops, uint32_t k, cons
       const uint2 ac = g.adj[c];
       const uint32_t *run = adj_list(g, ac);
       for (uint32_t i = lane; i < ac.y; i += 32) {
-        const uint32_t n = run[i];
+        const uint32_t n = run[i] & kIdMask;
         if (op.kind == 0) {
           const uint32_t code = vcand[n];
           for (uint32_t j = 0; j < op.nleaf; ++j)

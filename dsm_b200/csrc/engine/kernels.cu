@@ -11,6 +11,7 @@ __device__ __forceinline__ T ld_volatile(const T &x) {
   return *(const volatile T *)&x;
 }
 
+// Is {a, b} in the (label-major) graph: b's entry in the shorter of the two runs.
 __device__ __forceinline__ bool has_edge(const DevGraph &g, uint32_t a, uint32_t b) {
   uint2 aa = g.adj[a], bb = g.adj[b];
   if (bb.y < aa.y) {
@@ -21,9 +22,17 @@ __device__ __forceinline__ bool has_edge(const DevGraph &g, uint32_t a, uint32_t
     a = b;
     b = x;
   }
+  const uint32_t key = pack_entry(g.lab[b] & kLabelMask, b);
   const uint32_t *l = adj_list(g, aa);
-  uint32_t p = lower_bound_u32(l, aa.y, b);
-  return p < aa.y && l[p] == b;
+  uint32_t p = lower_bound_u32(l, aa.y, key);
+  return p < aa.y && l[p] == key;
+}
+
+// Slot offsets of x's run (d entries), by the warp that just rewrote it.
+__device__ void rebuild_loff(const DevGraph &g, uint32_t x, const uint32_t *run, uint32_t d) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t *t = g.loff + (size_t)x * (g.nlt + 1);
+  for (uint32_t s = lane; s <= g.nlt; s += 32) t[s] = s == g.nlt ? d : lower_bound_u32(run, d, s << kIdBits);
 }
 
 // ---------------------------------------------------------------------------
@@ -72,8 +81,9 @@ __device__ __forceinline__ uint8_t group_flag(const AdjUpdateArgs &A, uint32_t x
   return (lo < A.m && A.bkey[lo] == key) ? A.gflag[lo] : 0;
 }
 
-// Compacts the neighbours of source group [s, e) selected by `want` (and, for
-// inserts, not yet in the list) into dsel[s..s+k).  Returns k.
+// Compacts the entries of source group [s, e) selected by `want` (and, for
+// inserts, not yet in the run) into dsel[s..s+k), in entry order.  Returns k.
+// dkey holds x << 32 | entry of the neighbour, sorted.
 __device__ uint32_t select_group(const AdjUpdateArgs &A, uint32_t s, uint32_t e, uint32_t x,
                                  uint8_t want, bool skip_present, const uint32_t *L, uint32_t d) {
   const uint32_t lane = threadIdx.x & 31;
@@ -86,7 +96,7 @@ __device__ uint32_t select_group(const AdjUpdateArgs &A, uint32_t s, uint32_t e,
       unsigned long long key = A.dkey[j];
       y = (uint32_t)key;
       bool first = (j == s) || (A.dkey[j - 1] != key);
-      sel = first && (group_flag(A, x, y) & want);
+      sel = first && (group_flag(A, x, y & kIdMask) & want);
       if (sel && skip_present) {
         uint32_t p = lower_bound_u32(L, d, y);
         sel = !(p < d && L[p] == y);
@@ -140,6 +150,7 @@ __global__ void k_adj_insert(AdjUpdateArgs A) {
     const uint32_t *N = A.dsel + s;
     if (d + k <= c) {
       merge_down(L, d, N, k, L);
+      rebuild_loff(A.g, x, L, d + k);
       if (lane == 0) A.g.adj[x].y = d + k;
     } else {
       uint32_t need = d + k;
@@ -153,6 +164,7 @@ __global__ void k_adj_insert(AdjUpdateArgs A) {
       }
       uint32_t *out = A.g.arena + off16 * 4;
       merge_down(L, d, N, k, out);
+      rebuild_loff(A.g, x, out, need);
       if (lane == 0) {
         A.g.adj[x] = make_uint2((uint32_t)off16, need);
         A.g.cap[x] = ncap;
@@ -191,6 +203,7 @@ __global__ void k_adj_delete(AdjUpdateArgs A) {
       removed += __popc(md);
       __syncwarp();
     }
+    rebuild_loff(A.g, x, L, d - removed);
     if (lane == 0) A.g.adj[x].y = d - removed;
   }
 }

@@ -104,8 +104,12 @@ __device__ void finish_task(const MatchArgs &P) {
     atomicExch(&P.job_seq[t & (P.job_ring - 1)], t | kSeqDone);
 }
 
+// kLM: label-major runs with slot offsets (the engine's graph); otherwise
+// plain id-sorted runs.  srng[L][j]: for level L and backward neighbour j,
+// the range of j's run holding the label of level L (label-major only).
+template <bool kLM>
 __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t depth, uint32_t lo,
-                         uint32_t hi, uint32_t fval) {
+                         uint32_t hi, uint32_t fval, uint2 (*srng)[16]) {
   const uint32_t lane = threadIdx.x & 31;
   const QDev &Q = P.qd[qo >> 8];
   const uint32_t nq = Q.nq;
@@ -165,17 +169,37 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
     return;
   }
 
+  // Level L scans the run of its pivot: the backward neighbour with the
+  // fewest candidates (label-major: entries with L's label; plain: degree).
+  // [rlo, rhi) narrows the scan for a donated range (rhi = 0: all of it).
   uint32_t lv_base = 0, lv_pos = 0, lv_end = 0, lv_mask = 0, lv_chunk = 0, lv_pivot = 0;
   auto setup_level = [&](uint32_t L, uint32_t rlo, uint32_t rhi) {
-    uint32_t bnL = __shfl_sync(kFull, q_bn, L);
-    uint32_t key = ((bnL >> lane) & 1u) ? ((min(my_deg, 0x3FFFFFFu) << 5) | lane) : 0xFFFFFFFFu;
-    uint32_t mn = __reduce_min_sync(kFull, key);
-    uint32_t piv = mn & 31;
-    uint32_t poff = __shfl_sync(kFull, my_off, piv), pdeg = __shfl_sync(kFull, my_deg, piv);
+    const uint32_t bnL = __shfl_sync(kFull, q_bn, L);
+    const bool inb = (bnL >> lane) & 1u;
+    uint32_t a = 0, b = my_deg;
+    if constexpr (kLM) {
+      const uint32_t want = __shfl_sync(kFull, q_lab, L);
+      b = 0;
+      if (inb) {
+        if (want < P.g.nlt) {
+          const uint32_t *t = P.g.loff + (size_t)my_f * (P.g.nlt + 1) + want;
+          a = t[0];
+          b = t[1];
+        }
+      }
+      __syncwarp();  // lanes may still read this level's previous ranges
+      if (inb) srng[L][lane] = make_uint2(a, b);
+      __syncwarp();
+      alg += 8ull * __popc(bnL);
+    }
+    const uint32_t key = inb ? ((min(b - a, 0x3FFFFFFu) << 5) | lane) : 0xFFFFFFFFu;
+    const uint32_t piv = __reduce_min_sync(kFull, key) & 31;
+    const uint32_t poff = __shfl_sync(kFull, my_off, piv);
+    const uint32_t pa = __shfl_sync(kFull, a, piv), pb = __shfl_sync(kFull, b, piv);
     if (lane == L) {
       lv_base = poff;
-      lv_pos = rlo;
-      lv_end = rhi ? min(rhi, pdeg) : pdeg;
+      lv_pos = rhi ? rlo : pa;
+      lv_end = rhi ? min(rhi, pb) : pb;
       lv_mask = 0;
       lv_pivot = piv;
     }
@@ -198,12 +222,22 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
       const uint32_t *run = P.g.arena + (uint64_t)base * 4;
       const uint32_t i = pos + lane;
       bool ok = i < end;
-      uint32_t w = ok ? run[i] : 0;
-      uint32_t lw = ok ? P.g.lab[w] : 0;
+      const uint32_t e = ok ? run[i] : 0;  // entry (label-major) or id
+      const uint32_t w = kLM ? (e & kIdMask) : e;
       const uint32_t want = __shfl_sync(kFull, q_lab, L);
-      ok = ok && ((lw & kLabelMask) == want);
-      for (uint32_t j = 0; j < L; ++j) {
-        uint32_t fj = __shfl_sync(kFull, my_f, j);
+      uint32_t lw = 0;
+      if constexpr (kLM) {
+        if (want >= 31) {  // slot 31 holds every label >= 31
+          lw = ok ? P.g.lab[w] : 0;
+          ok = ok && ((lw & kLabelMask) == want);
+        }
+      } else {
+        lw = ok ? P.g.lab[w] : 0;
+        ok = ok && ((lw & kLabelMask) == want);
+      }
+      // injectivity: only earlier positions with the same label can hold w
+      for (uint32_t same = __ballot_sync(kFull, lane < L && q_lab == want); same; same &= same - 1) {
+        const uint32_t fj = __shfl_sync(kFull, my_f, __ffs(same) - 1);
         ok = ok && (w != fj);
       }
       if (bitmap) {
@@ -216,13 +250,27 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
       while (others) {
         uint32_t j = __ffs(others) - 1;
         others &= others - 1;
-        uint32_t oj = __shfl_sync(kFull, my_off, j), dj = __shfl_sync(kFull, my_deg, j);
-        if (ok) {
-          const uint32_t *lst = P.g.arena + (uint64_t)oj * 4;
-          uint32_t p = lower_bound_u32(lst, dj, w);
-          ok = p < dj && lst[p] == w;
-          ++probes;
+        const uint32_t oj = __shfl_sync(kFull, my_off, j);
+        if constexpr (kLM) {
+          const uint2 r = srng[L][j];
+          if (ok) {
+            const uint32_t *lst = P.g.arena + (uint64_t)oj * 4;
+            const uint32_t p = r.x + lower_bound_u32(lst + r.x, r.y - r.x, e);
+            ok = p < r.y && lst[p] == e;
+            ++probes;
+          }
+        } else {
+          const uint32_t dj = __shfl_sync(kFull, my_deg, j);
+          if (ok) {
+            const uint32_t *lst = P.g.arena + (uint64_t)oj * 4;
+            uint32_t p = lower_bound_u32(lst, dj, w);
+            ok = p < dj && lst[p] == w;
+            ++probes;
+          }
         }
+      }
+      if constexpr (kLM) {
+        if (want < 31) lw = ok ? P.g.lab[w] : 0;  // touch bit of the survivors
       }
       if (__any_sync(kFull, ok && (lw >> 31))) {
         uint32_t bits = bnL;
@@ -234,7 +282,7 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
         }
       }
       uint32_t m = __ballot_sync(kFull, ok);
-      alg += 8ull * min(32u, end - pos) + 4ull * __reduce_add_sync(kFull, probes);
+      alg += (kLM ? 4ull : 8ull) * min(32u, end - pos) + 4ull * __reduce_add_sync(kFull, probes);
       if (lane == L) {
         lv_pos = pos + 32;
         lv_chunk = pos;
@@ -317,6 +365,7 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
                   uint32_t b = __ffs(bits) - 1;
                   bits &= bits - 1;
                   cw = P.g.arena[(uint64_t)pbase * 4 + pchunk + b];
+                  if constexpr (kLM) cw &= kIdMask;
                   jdepth = p + 1;
                 } else {
                   jdepth = p;
@@ -352,7 +401,8 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
     const uint32_t b = __ffs(mask) - 1;
     const uint32_t chunk = __shfl_sync(kFull, lv_chunk, L);
     const uint32_t base = __shfl_sync(kFull, lv_base, L);
-    const uint32_t w = P.g.arena[(uint64_t)base * 4 + chunk + b];
+    uint32_t w = P.g.arena[(uint64_t)base * 4 + chunk + b];
+    if constexpr (kLM) w &= kIdMask;
     if (lane == L) {
       lv_mask = mask & (mask - 1);
       my_f = w;
@@ -382,7 +432,9 @@ __global__ void k_sched_init(Sched *sc, unsigned long long seed_cap, unsigned lo
   }
 }
 
+template <bool kLM>
 __global__ void __launch_bounds__(256) k_match(MatchArgs P) {
+  __shared__ uint2 s_rng[kLM ? 8 : 1][16][16];
   const uint32_t lane = threadIdx.x & 31;
   bool seeds_done = false;
   while (true) {
@@ -414,7 +466,7 @@ __global__ void __launch_bounds__(256) k_match(MatchArgs P) {
       hi = __shfl_sync(kFull, word, 4);
       fval = __shfl_sync(kFull, word, (lane + 8) & 31);
     }
-    run_task(P, upd, qo, depth, lo, hi, fval);
+    run_task<kLM>(P, upd, qo, depth, lo, hi, fval, s_rng[kLM ? (threadIdx.x >> 5) : 0]);
     finish_task(P);
   }
 }
@@ -427,13 +479,15 @@ void launch_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long lon
 }
 
 void launch_match(const MatchArgs &a, int blocks, cudaStream_t s) {
-  k_match<<<blocks, 256, 0, s>>>(a);
+  if (a.g.loff) k_match<true><<<blocks, 256, 0, s>>>(a);
+  else k_match<false><<<blocks, 256, 0, s>>>(a);
 }
 
 int match_max_blocks_per_sm() {
-  int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_match, 256, 0);
-  return n;
+  int n = 0, m = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_match<true>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_match<false>, 256, 0);
+  return n < m ? n : m;
 }
 
 }  // namespace dsm
