@@ -143,7 +143,7 @@ int Engine::init(int dev, size_t mem_budget) {
   ev_pool.resize(8, nullptr);
   for (auto &ev : ev_pool) CK(cudaEventCreate(&ev));
   int per_sm = match_max_blocks_per_sm();
-  match_blocks_per_sm = std::max(1, std::min(per_sm, 4));
+  match_blocks_per_sm = std::max(1, std::min(per_sm, 8));
   // small fixed buffers
   if (int rc = dalloc(d_sched, sizeof(Sched))) return rc;
   if (int rc = dalloc(d_arena_top, 256)) return rc;

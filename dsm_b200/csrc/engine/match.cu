@@ -137,8 +137,8 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
     uint32_t cnt = __popc(m);
     if (cnt == 0) return;
     task_cnt += cnt;
-    alg += 4ull * (nq + 1) * cnt;
     if (!P.list) return;
+    alg += 4ull * (nq + 1) * cnt;  // the tuple and its segment id
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(&P.sc->out_count.v, (unsigned long long)cnt);
     base = __shfl_sync(kFull, base, 0);
@@ -432,8 +432,13 @@ __global__ void k_sched_init(Sched *sc, unsigned long long seed_cap, unsigned lo
   }
 }
 
+// Resident blocks per SM the register allocation is sized for.
+#ifndef DSM_MATCH_MIN_BLOCKS
+#define DSM_MATCH_MIN_BLOCKS 5
+#endif
+
 template <bool kLM>
-__global__ void __launch_bounds__(256) k_match(MatchArgs P) {
+__global__ void __launch_bounds__(256, DSM_MATCH_MIN_BLOCKS) k_match(MatchArgs P) {
   __shared__ uint2 s_rng[kLM ? 8 : 1][16][16];
   const uint32_t lane = threadIdx.x & 31;
   bool seeds_done = false;
