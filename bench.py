@@ -226,6 +226,130 @@ def run_ours(args, rank, world):
     return line
 
 
+def run_serve(args):
+    """Serving comparison on the config-4 stream (R-MAT, 32 uniform labels,
+    lognormal batch sizes with median 512, 60% inserts): the same requests
+    through three forms, each from the same initial graph.
+      plain:   one engine per query, one launch per query per batch, in turn;
+      batched: one engine, all queries in one launch per batch;
+      served:  one engine with the serving loop (continuous batching).
+    Phase 1 (burst): every request at t=0 -> throughput.  Phase 2 (the next
+    requests): Poisson arrivals at 70% of the batched form's burst request
+    rate -> p50 / p99 latency from arrival to results readable on the host."""
+    import torch
+
+    import dsm_b200 as d
+    torch.cuda.set_device(0)
+    K = args.serve_requests
+    scale = args.scale if args.scale else -6
+    t0 = time.time()
+    w = d.Workload(4, scale_log2=scale, num_batches=2 * K)
+    gen_s = time.time() - t0
+    reqs = list(w.batches())[:2 * K]
+    burst, poisson = reqs[:K], reqs[K:]
+    # 8-10-vertex random-walk queries through the R-MAT hubs carry up to
+    # 10^11 embeddings per request at this scale; the serving comparison uses
+    # the pool's queries of at most 7 vertices
+    qs = [q for q in w.queries if q.nv <= 7][:args.serve_queries]
+    print(f"[serve] workload in {gen_s:.1f} s: {w.nv} vertices, {len(w.edges)} edges, {len(qs)} queries, "
+          f"request sizes median {int(np.median([len(r) for r in reqs]))} max {max(len(r) for r in reqs)}",
+          file=sys.stderr, flush=True)
+
+    def engine(qlist):
+        e = d.Engine(0)
+        e.set_option(d.OPT_LIST, args.list)
+        e.load_graph_edges(w.nv, w.labels, w.edges)
+        return e, [e.register(q) for q in qlist]
+
+    def summarize(lat_ms, matches, updates, span_s):
+        lat = np.sort(np.asarray(lat_ms))
+        return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "matches_per_sec": matches / span_s, "updates_per_sec": updates / span_s, "span_s": span_s,
+                "matches": int(matches)}
+
+    def run_sync(engines, arrivals, batch_list):
+        """One request at a time, in arrival order, through every engine."""
+        lat, matches, upd = [], 0, 0
+        torch.cuda.synchronize()
+        base = time.perf_counter()
+        for a, b in zip(arrivals, batch_list):
+            now = time.perf_counter() - base
+            if now < a:
+                time.sleep(a - now)
+            for e, _ in engines:
+                r = e.run_batch(b)
+                matches += int(r.counts.sum())
+            lat.append((time.perf_counter() - base - a) * 1e3)
+            upd += len(b)
+        return summarize(lat, matches, upd, time.perf_counter() - base)
+
+    def run_served(e, arrivals, batch_list):
+        bids = []
+        base = time.perf_counter()
+
+        def submitter():
+            for a, b in zip(arrivals, batch_list):
+                now = time.perf_counter() - base
+                if now < a:
+                    time.sleep(a - now)
+                bids.append(e.submit(b))
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat, matches, upd, merged = [], 0, 0, []
+        for k in range(len(batch_list)):
+            while len(bids) <= k:
+                time.sleep(0.0002)
+            t = e.timing(bids[k])
+            r = e.results(bids[k])
+            lat.append(t["total_ms"])
+            merged.append(t["merged_requests"])
+            matches += int(r.counts.sum())
+            upd += r.num_updates
+        th.join()
+        out = summarize(lat, matches, upd, time.perf_counter() - base)
+        out["mean_requests_per_device_batch"] = float(np.mean(merged))
+        return out
+
+    arms = {}
+    sampler = ClockSampler(0)
+    sampler.start()
+    # batched first: its burst rate sets the Poisson rate
+    e, _ = engine(qs)
+    arms["batched"] = {"burst": run_sync([(e, None)], np.zeros(K), burst)}
+    rate = 0.7 * K / arms["batched"]["burst"]["span_s"]
+    arrivals = np.cumsum(np.random.default_rng(4).exponential(1.0 / rate, K))
+    arms["batched"]["poisson"] = run_sync([(e, None)], arrivals, poisson)
+    e.close()
+    print(f"[serve] batched done; Poisson rate {rate:.1f} requests/s", file=sys.stderr, flush=True)
+    e, _ = engine(qs)
+    e.serve_start(args.serve_merge)
+    arms["served"] = {"burst": run_served(e, np.zeros(K), burst), "poisson": run_served(e, arrivals, poisson)}
+    e.serve_stop()
+    e.close()
+    print("[serve] served done", file=sys.stderr, flush=True)
+    engines = [engine([q]) for q in qs]
+    arms["plain"] = {"burst": run_sync(engines, np.zeros(K), burst), "poisson": run_sync(engines, arrivals, poisson)}
+    for e, _ in engines:
+        e.close()
+    clocks = sampler.stop()
+    for k in ("batched", "served", "plain"):
+        assert arms[k]["burst"]["matches"] == arms["batched"]["burst"]["matches"], "forms disagree"
+        assert arms[k]["poisson"]["matches"] == arms["batched"]["poisson"]["matches"], "forms disagree"
+    sv = arms["served"]["poisson"]
+    return {
+        "metric": "served_p99_batch_latency_ms", "value": sv["p99_ms"], "unit": "ms", "n_gpus": 1,
+        "higher_is_better": False, "dtype": "u32", "data": "synthetic (seeded R-MAT graph, generated stream)",
+        "config": {"workload": f"config4 stream on R-MAT(0.57,0.19,0.19) |V|=2^{24 + scale}, "
+                               f"|E|=2^{28 + scale}, 32 uniform labels, {len(qs)} queries of 4-7 vertices "
+                               f"(the first of the 64-query pool of 4-10 vertices with at most 7), "
+                               f"lognormal request sizes (median 512), 60% inserts",
+                   "requests_per_phase": K, "poisson_rate_per_s": rate, "listing": bool(args.list),
+                   "max_merge_updates": args.serve_merge or 65536},
+        "arms": arms, "clocks": clocks, "gen_seconds": gen_s,
+    }
+
+
 def cpu_baseline(w, batch, sample):
     """The oracle (CPU restatement, one thread) on the first `sample` updates
     of the first timed batch for each query."""
@@ -287,9 +411,17 @@ def main():
     ap.add_argument("--scale", type=int, default=0, help="log2 shrink of the graph (0 = config size)")
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="step", choices=["step", "serve"],
+                    help="serve: served vs batched vs plain on the config-4 request stream")
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-queries", type=int, default=16)
+    ap.add_argument("--serve-merge", type=int, default=0)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.mode == "serve":
+        print(json.dumps(run_serve(args)), flush=True)
+        return
     if args.impl == "reference":
         # CPU arm: rank 0 alone runs; other ranks exit without work
         line = run_reference(args, rank)

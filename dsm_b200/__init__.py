@@ -19,7 +19,7 @@ ERR = {1: "PARSE", 2: "OOM", 3: "OVERFLOW", 4: "TIMEOUT", 5: "LIMIT", 6: "ARG", 
        9: "NOT_FOUND"}
 
 OPT_LIST, OPT_FILTER, OPT_RESULT_CAP, OPT_WARPS_PER_SM, OPT_DONATE, OPT_TIMEOUT_MS, OPT_LABEL_QUIRK, OPT_SORT, \
-    OPT_LIST_LIMIT = range(1, 10)
+    OPT_LIST_LIMIT, OPT_MEM_BUDGET = range(1, 11)
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is not built; run `python dsm_b200/build.py`")
@@ -44,8 +44,13 @@ class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("batches", "updates", "matches", "seeds", "donations", "steals",
                                           "relocations", "result_regrows", "alg_bytes")] + \
                [(n, C.c_double) for n in ("last_batch_ms", "last_match_ms", "last_filter_ms", "last_update_ms",
-                                          "last_sort_ms")] + [("device_bytes_in_use", C.c_uint64),
-                                                              ("kernel_launches", C.c_uint64)]
+                                          "last_sort_ms")] + [(n, C.c_uint64) for n in (
+                   "device_bytes_in_use", "kernel_launches", "query_bytes", "live_queries")]
+
+
+class BatchTiming(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("queue_ms", "service_ms", "total_ms", "device_ms")] + \
+               [(n, C.c_uint32) for n in ("merged_requests", "merged_updates")]
 
 
 def _sig(name, res, *args):
@@ -75,6 +80,12 @@ _sig("dsm_batch_wait", C.c_int, P, C.c_uint64)
 _sig("dsm_batch_results", C.c_int, P, C.c_uint64, C.POINTER(ResultView))
 _sig("dsm_batch_release", C.c_int, P, C.c_uint64)
 _sig("dsm_engine_stats", C.c_int, P, C.POINTER(Stats))
+_sig("dsm_batch_timing_get", C.c_int, P, C.c_uint64, C.POINTER(BatchTiming))
+_sig("dsm_serve_start", C.c_int, P, C.c_uint32)
+_sig("dsm_serve_stop", C.c_int, P)
+_sig("dsm_query_register_async", C.c_int, P, u32p, u32p, u32p, C.c_uint32, C.POINTER(C.c_uint64))
+_sig("dsm_query_retire_async", C.c_int, P, C.c_uint32, C.POINTER(C.c_uint64))
+_sig("dsm_query_admission", C.c_int, P, C.c_uint64, C.c_int64, C.POINTER(C.c_uint32))
 _sig("dsm_text_read", C.c_int, C.c_char_p, C.c_int, C.POINTER(P), C.c_char_p, C.c_size_t)
 _sig("dsm_text_free", None, P)
 for _n in ("nv", "ne", "num_batches", "num_updates"):
@@ -346,6 +357,40 @@ class Engine:
 
     def run_batch(self, updates):
         return self.results(self.submit(updates))
+
+    def wait(self, bid):
+        self._ck(lib.dsm_batch_wait(self._h, bid))
+
+    def timing(self, bid):
+        t = BatchTiming()
+        self._ck(lib.dsm_batch_timing_get(self._h, bid, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in BatchTiming._fields_}
+
+    # serving loop
+    def serve_start(self, max_merge_updates=0):
+        self._ck(lib.dsm_serve_start(self._h, max_merge_updates))
+
+    def serve_stop(self):
+        self._ck(lib.dsm_serve_stop(self._h))
+
+    def register_async(self, q):
+        t = C.c_uint64()
+        self._ck(lib.dsm_query_register_async(self._h, q.offsets, q.nbrs, q.labels, q.nv, C.byref(t)))
+        return t.value
+
+    def retire_async(self, qid):
+        t = C.c_uint64()
+        self._ck(lib.dsm_query_retire_async(self._h, qid, C.byref(t)))
+        return t.value
+
+    def admission(self, ticket, timeout_ms=-1):
+        """qid once admitted; None while the registration still waits."""
+        qid = C.c_uint32()
+        rc = lib.dsm_query_admission(self._h, ticket, int(timeout_ms), C.byref(qid))
+        if rc == 4:  # DSM_ERR_TIMEOUT
+            return None
+        self._ck(rc)
+        return qid.value
 
     def stats(self):
         s = Stats()

@@ -28,8 +28,8 @@ LIB_SOURCES = [
     "engine/kernels.cu",
     "engine/match.cu",
     "engine/filter.cu",
-    
     "engine/engine.cu",
+    "engine/serve.cu",
     "engine/abi.cu",
     "engine/noalloc.cu",
     "host/gen.cpp",

@@ -80,6 +80,12 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
       if (value <= 0) return E.fail(DSM_ERR_ARG, "listing limit must be positive");
       E.list_limit_bytes = (uint64_t)value;
       return DSM_OK;
+    case DSM_OPT_MEM_BUDGET:
+      if (value <= 0 || (uint64_t)value < E.bytes_in_use)
+        return E.fail(DSM_ERR_ARG, "budget must cover the bytes in use");
+      E.budget = (size_t)value;
+      E.admit_pending();
+      return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");
 }
@@ -98,6 +104,7 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_LABEL_QUIRK: *value = E.label_quirk; return DSM_OK;
     case DSM_OPT_SORT: *value = E.sort_results; return DSM_OK;
     case DSM_OPT_LIST_LIMIT: *value = (int64_t)E.list_limit_bytes; return DSM_OK;
+    case DSM_OPT_MEM_BUDGET: *value = (int64_t)E.budget; return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");
 }
@@ -220,8 +227,42 @@ int dsm_batch_submit(dsm_engine *e, const dsm_update *ups, uint32_t n, uint64_t 
 
 int dsm_batch_wait(dsm_engine *e, uint64_t batch_id) {
   ENGINE_OR_ARG(e);
-  std::lock_guard<std::mutex> lk(e->e.mu);
-  return e->e.results.count(batch_id) ? DSM_OK : e->e.fail(DSM_ERR_NOT_FOUND, "no such batch");
+  return e->e.wait_batch(batch_id);
+}
+
+int dsm_batch_timing_get(dsm_engine *e, uint64_t batch_id, dsm_batch_timing *t) {
+  ENGINE_OR_ARG(e);
+  if (!t) return DSM_ERR_ARG;
+  return e->e.timing(batch_id, t);
+}
+
+int dsm_serve_start(dsm_engine *e, uint32_t max_merge_updates) {
+  ENGINE_OR_ARG(e);
+  return e->e.serve_start(max_merge_updates);
+}
+
+int dsm_serve_stop(dsm_engine *e) {
+  ENGINE_OR_ARG(e);
+  return e->e.serve_stop();
+}
+
+int dsm_query_register_async(dsm_engine *e, const uint32_t *q_offsets, const uint32_t *q_nbrs,
+                             const uint32_t *q_labels, uint32_t nq, uint64_t *ticket) {
+  ENGINE_OR_ARG(e);
+  if (!q_offsets || !q_nbrs || !q_labels || !ticket) return DSM_ERR_ARG;
+  return e->e.register_async(q_offsets, q_nbrs, q_labels, nq, ticket);
+}
+
+int dsm_query_retire_async(dsm_engine *e, uint32_t qid, uint64_t *ticket) {
+  ENGINE_OR_ARG(e);
+  if (!ticket) return DSM_ERR_ARG;
+  return e->e.retire_async(qid, ticket);
+}
+
+int dsm_query_admission(dsm_engine *e, uint64_t ticket, int64_t timeout_ms, uint32_t *qid) {
+  ENGINE_OR_ARG(e);
+  if (!qid) return DSM_ERR_ARG;
+  return e->e.admission(ticket, timeout_ms, qid);
 }
 
 int dsm_batch_results(dsm_engine *e, uint64_t batch_id, dsm_result_view *view) {
@@ -241,6 +282,12 @@ int dsm_engine_stats(dsm_engine *e, dsm_stats *s) {
   std::lock_guard<std::mutex> lk(e->e.mu);
   *s = e->e.stats;
   s->device_bytes_in_use = e->e.bytes_in_use;
+  s->query_bytes = s->live_queries = 0;
+  for (const auto &q : e->e.slots)
+    if (q.live) {
+      s->query_bytes += q.foot;
+      s->live_queries++;
+    }
   return DSM_OK;
 }
 

@@ -102,6 +102,7 @@ int Engine::halloc(HostBuf &b, size_t bytes) {
 }
 
 Engine::~Engine() {
+  serve_stop();
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
   for (DevBuf *b : all_dev_bufs()) dfree(*b);
@@ -292,17 +293,32 @@ int Engine::export_graph(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entrie
 // ---------------------------------------------------------------------------
 // Queries
 // ---------------------------------------------------------------------------
-int Engine::register_query(const uint32_t *qoff, const uint32_t *qnbr, const uint32_t *qlab, uint32_t nq,
-                           uint32_t *qid) {
-  std::lock_guard<std::mutex> lk(mu);
-  QueryPlan plan;
-  std::string err;
-  int rc = plan_query(nq, qoff, qnbr, qlab, plan, err);
-  if (rc) return fail(rc, err);
-  // admission: descriptor + filter bitmaps + encodings
-  size_t foot = sizeof(QDev) + plan.orders.size() * sizeof(OrderRec);
-  if (graph_loaded) foot += (size_t)nq * ((nv + 31) / 32) * 4 + (size_t)nv * plan.enc_words * 4 + (size_t)nv * nq * 4;
-  if (bytes_in_use + foot > budget)
+// Device bytes a query is charged at admission: its descriptor and orders,
+// and (for the candidate filter) bitmaps, LDF/NLF masks and encodings.
+size_t Engine::query_footprint(const QueryPlan &p) const {
+  size_t foot = sizeof(QDev) + p.orders.size() * sizeof(OrderRec);
+  if (graph_loaded)
+    foot += (size_t)p.nq * ((nv + 31) / 32) * 4 + (size_t)nv * (8 + 4 * std::max<uint32_t>(p.enc_words, 1));
+  return foot;
+}
+
+size_t Engine::query_bytes_allocated() const {
+  size_t b = 0;
+  for (const Slot &q : slots) b += q.bitmap.bytes + q.filter_scratch.bytes + q.filter_plan.bytes;
+  return b;
+}
+
+// Admission against the budget: engine bytes not owned by queries + the
+// footprints of the admitted queries + this one.  *fits_later: it would fit
+// once every other query retired.
+int Engine::admit(QueryPlan &plan, uint32_t *qid, bool *fits_later) {
+  const size_t foot = query_footprint(plan);
+  const size_t base = bytes_in_use - std::min(bytes_in_use, query_bytes_allocated());
+  size_t charged = 0;
+  for (const Slot &q : slots)
+    if (q.live) charged += q.foot;
+  if (fits_later) *fits_later = base + foot <= budget;
+  if (base + charged + foot > budget)
     return fail(DSM_ERR_OOM, "query admission: footprint " + std::to_string(foot) + " bytes exceeds the budget");
   uint32_t id = (uint32_t)slots.size();
   for (uint32_t i = 0; i < slots.size(); ++i)
@@ -310,25 +326,62 @@ int Engine::register_query(const uint32_t *qoff, const uint32_t *qnbr, const uin
       id = i;
       break;
     }
-  if (id == slots.size()) slots.emplace_back();
   if (id >= (1u << 23)) return fail(DSM_ERR_LIMIT, "too many queries");
+  if (id == slots.size()) slots.emplace_back();
   Slot &s = slots[id];
   s.live = true;
   s.plan = std::move(plan);
   s.filter_dirty = true;
+  s.foot = foot;
   queries_dirty = true;
   *qid = id;
   return DSM_OK;
 }
 
-int Engine::retire_query(uint32_t qid) {
+int Engine::register_query(const uint32_t *qoff, const uint32_t *qnbr, const uint32_t *qlab, uint32_t nq,
+                           uint32_t *qid) {
+  bool serving;
+  {
+    std::lock_guard<std::mutex> q(srv.qmu);
+    serving = srv.running;
+  }
+  if (serving) {  // through the queue, in order with the batches
+    uint64_t ticket = 0;
+    if (int rc = register_async(qoff, qnbr, qlab, nq, &ticket)) return rc;
+    return admission(ticket, -1, qid);
+  }
   std::lock_guard<std::mutex> lk(mu);
+  QueryPlan plan;
+  std::string err;
+  if (int rc = plan_query(nq, qoff, qnbr, qlab, plan, err)) return fail(rc, err);
+  return admit(plan, qid, nullptr);
+}
+
+int Engine::retire_query(uint32_t qid) {
+  bool serving;
+  {
+    std::lock_guard<std::mutex> q(srv.qmu);
+    serving = srv.running;
+  }
+  if (serving) {
+    uint64_t ticket = 0;
+    if (int rc = retire_async(qid, &ticket)) return rc;
+    uint32_t dummy = 0;
+    return admission(ticket, -1, &dummy);
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  return retire_locked(qid);
+}
+
+int Engine::retire_locked(uint32_t qid) {
   if (qid >= slots.size() || !slots[qid].live) return fail(DSM_ERR_NOT_FOUND, "no such query");
   Slot &s = slots[qid];
   s.live = false;
   dfree(s.bitmap);
   dfree(s.filter_scratch);
+  dfree(s.filter_plan);
   s.plan = QueryPlan();
+  s.foot = 0;
   queries_dirty = true;
   return DSM_OK;
 }
@@ -394,20 +447,85 @@ int Engine::upload_qd() {
 // ---------------------------------------------------------------------------
 // Batches
 // ---------------------------------------------------------------------------
-int Engine::submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id) {
-  std::lock_guard<std::mutex> lk(mu);
+int Engine::check_updates(const dsm_update *ups, uint32_t n) {
   if (!graph_loaded) return fail(DSM_ERR_STATE, "no graph loaded");
   if (n >= (1u << 30)) return fail(DSM_ERR_LIMIT, "batch larger than 2^30 updates");
   for (uint32_t i = 0; i < n; ++i)
     if (ups[i].src >= nv || ups[i].dst >= nv) return fail(DSM_ERR_ARG, "update names a vertex >= num_v");
+  return DSM_OK;
+}
+
+int Engine::submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id) {
+  {
+    std::unique_lock<std::mutex> q(srv.qmu);
+    if (srv.running) {
+      if (srv.stopping) return fail(DSM_ERR_STATE, "the serving loop is stopping");
+      q.unlock();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        if (int rc = check_updates(ups, n)) return rc;
+      }
+      Request r;
+      r.kind = kReqBatch;
+      r.ups.assign(ups, ups + n);
+      r.t_submit = std::chrono::steady_clock::now();
+      q.lock();
+      r.id = next_batch_id++;
+      *batch_id = r.id;
+      srv.queue.push_back(std::move(r));
+      srv.work_cv.notify_one();
+      return DSM_OK;
+    }
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (int rc = check_updates(ups, n)) return rc;
   CK(cudaSetDevice(device));
+  const auto t0 = std::chrono::steady_clock::now();
   auto res = std::make_unique<BatchResult>();
   int rc = run_batch(ups, n, *res);
   if (rc) return rc;
-  uint64_t id = next_batch_id++;
+  const uint64_t id = next_batch_id++;
   res->id = id;
-  results[id] = std::move(res);
+  res->service_ms = res->total_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  res->merged_updates = n;
+  {
+    std::lock_guard<std::mutex> r(rmu);
+    results[id] = std::move(res);
+  }
+  {
+    std::lock_guard<std::mutex> q(srv.qmu);
+    srv.done.insert(id);
+  }
   *batch_id = id;
+  return DSM_OK;
+}
+
+// Blocks until batch `id` is done; its status.
+int Engine::wait_batch(uint64_t id) {
+  std::unique_lock<std::mutex> q(srv.qmu);
+  if (id == 0 || id >= next_batch_id) return fail(DSM_ERR_NOT_FOUND, "no such batch");
+  srv.done_cv.wait(q, [&] { return srv.done.count(id) != 0; });
+  auto f = srv.failed.find(id);
+  if (f != srv.failed.end()) {
+    last_error = f->second.msg;
+    return f->second.rc;
+  }
+  return DSM_OK;
+}
+
+int Engine::timing(uint64_t id, dsm_batch_timing *t) {
+  if (int rc = wait_batch(id)) return rc;
+  std::lock_guard<std::mutex> lk(rmu);
+  auto it = results.find(id);
+  if (it == results.end()) return fail(DSM_ERR_NOT_FOUND, "no such batch (released?)");
+  const BatchResult &R = *it->second;
+  t->queue_ms = R.queue_ms;
+  t->service_ms = R.service_ms;
+  t->total_ms = R.total_ms;
+  t->device_ms = R.device_ms;
+  t->merged_requests = R.merged_requests;
+  t->merged_updates = R.merged_updates;
   return DSM_OK;
 }
 
@@ -801,7 +919,8 @@ int Engine::query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us) {
 }
 
 int Engine::view(uint64_t id, dsm_result_view *v) {
-  std::lock_guard<std::mutex> lk(mu);
+  if (int rc = wait_batch(id)) return rc;
+  std::lock_guard<std::mutex> lk(rmu);
   auto it = results.find(id);
   if (it == results.end()) return fail(DSM_ERR_NOT_FOUND, "no such batch (released?)");
   BatchResult &R = *it->second;
@@ -819,7 +938,7 @@ int Engine::view(uint64_t id, dsm_result_view *v) {
 }
 
 int Engine::release(uint64_t id) {
-  std::lock_guard<std::mutex> lk(mu);
+  std::lock_guard<std::mutex> lk(rmu);
   auto it = results.find(id);
   if (it == results.end()) return fail(DSM_ERR_NOT_FOUND, "no such batch");
   results.erase(it);

@@ -3,11 +3,17 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <cstdint>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/dsm.h"
@@ -35,6 +41,7 @@ struct Slot {
   DevBuf filter_plan;     // QFilterDesc + op list
   uint32_t filter_nops = 0;
   bool filter_dirty = true;  // plan or sizes must be (re)uploaded
+  size_t foot = 0;           // device bytes charged to this query at admission
 };
 
 struct BatchResult {
@@ -47,6 +54,44 @@ struct BatchResult {
   int listed = 1;
   double device_ms = 0, match_ms = 0, host_prep_ms = 0;
   uint64_t alg_bytes = 0, matches = 0;
+  // served timing: submit -> start of the device batch -> results readable
+  double queue_ms = 0, service_ms = 0, total_ms = 0;
+  uint32_t merged_requests = 1, merged_updates = 0;
+};
+
+// A request of the serving loop, in submission order.
+enum ReqKind { kReqBatch = 0, kReqRegister = 1, kReqRetire = 2 };
+struct Request {
+  int kind = kReqBatch;
+  uint64_t id = 0;  // batch id, or the ticket of a registration / retirement
+  std::vector<dsm_update> ups;
+  QueryPlan plan;   // registration (planned and validated at submit)
+  uint32_t qid = 0; // retirement
+  std::chrono::steady_clock::time_point t_submit;
+};
+struct Outcome {
+  int rc = DSM_OK;
+  uint32_t qid = 0;
+  std::string msg;
+};
+
+// Serving loop: one worker thread drains the request queue.  Consecutive
+// batches are merged into one device batch of at most max_merge updates;
+// registrations and retirements take effect between device batches, in
+// submission order.  A registration whose footprint does not fit now waits
+// (FIFO) until retirements free memory.
+struct Server {
+  bool running = false, stopping = false;
+  std::thread worker;
+  std::mutex qmu;  // queue, pending, tickets, done, failed
+  std::condition_variable work_cv, done_cv;
+  std::deque<Request> queue;
+  std::deque<Request> pending;
+  std::map<uint64_t, Outcome> tickets;
+  std::set<uint64_t> done;               // batches whose results (or failure) are final
+  std::map<uint64_t, Outcome> failed;
+  uint32_t max_merge = 65536;
+  uint64_t next_ticket = 1;
 };
 
 struct Engine {
@@ -95,10 +140,12 @@ struct Engine {
       d_job_seq, d_out_seg, d_out_tup, d_segcnt, d_misc;
   HostBuf h_stage, h_sched, h_segcnt, h_vtp, h_out_seg, h_out_tup;
 
-  // results
+  // results (own lock: a waiter reads batch k while batch k + 1 runs)
+  std::mutex rmu;
   std::map<uint64_t, std::unique_ptr<BatchResult>> results;
-  uint64_t next_batch_id = 1;
+  std::atomic<uint64_t> next_batch_id{1};
   dsm_stats stats{};
+  Server srv;
 
   ~Engine();
   int init(int device, size_t budget);
@@ -116,6 +163,10 @@ struct Engine {
 
   int register_query(const uint32_t *qoff, const uint32_t *qnbr, const uint32_t *qlab, uint32_t nq, uint32_t *qid);
   int retire_query(uint32_t qid);
+  size_t query_footprint(const QueryPlan &p) const;
+  size_t query_bytes_allocated() const;
+  int admit(QueryPlan &plan, uint32_t *qid, bool *fits_later);  // mu held
+  int retire_locked(uint32_t qid);                              // mu held
   int sync_queries();
   int upload_qd();
   int run_filters();
@@ -123,10 +174,25 @@ struct Engine {
   int launch_filter(uint32_t id, int mode);
   int query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);
 
+  int check_updates(const dsm_update *ups, uint32_t n);
   int submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id);
   int run_batch(const dsm_update *ups, uint32_t n, BatchResult &R);
+  int wait_batch(uint64_t id);
   int view(uint64_t id, dsm_result_view *v);
   int release(uint64_t id);
+  int timing(uint64_t id, dsm_batch_timing *t);
+
+  // serving loop (serve.cu)
+  int serve_start(uint32_t max_merge);
+  int serve_stop();
+  int register_async(const uint32_t *qoff, const uint32_t *qnbr, const uint32_t *qlab, uint32_t nq,
+                     uint64_t *ticket);
+  int retire_async(uint32_t qid, uint64_t *ticket);
+  int admission(uint64_t ticket, int64_t timeout_ms, uint32_t *qid);
+  void worker_loop();
+  Outcome handle_control(Request &r);
+  void admit_pending();
+  void run_merged(std::vector<Request> &reqs);
 };
 
 }  // namespace dsm

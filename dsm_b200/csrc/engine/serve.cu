@@ -1,0 +1,258 @@
+// Serving loop of the engine: a worker thread that drains the request queue
+// with continuous batching (no counterpart in the reference, whose main loop
+// serves one query and one batch at a time, main.cu:152-347).
+//
+// Batches queued back to back run as one device batch.  That is exact: the
+// batch pipeline gives every update the graph state after (insert) or before
+// (delete) it in array order, so concatenating requests changes no update's
+// result; only the device work per launch grows.  Registrations and
+// retirements are barriers between device batches.  Lock order: mu (engine
+// state, device work) before rmu (results) or qmu (queue); the worker never
+// holds qmu while it takes mu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+#include "engine_internal.h"
+
+namespace dsm {
+
+namespace {
+double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+}  // namespace
+
+int Engine::serve_start(uint32_t max_merge) {
+  std::lock_guard<std::mutex> q(srv.qmu);
+  if (srv.running) return fail(DSM_ERR_STATE, "the serving loop is already running");
+  srv.max_merge = max_merge ? max_merge : 65536;
+  srv.stopping = false;
+  srv.running = true;
+  srv.worker = std::thread([this] { worker_loop(); });
+  return DSM_OK;
+}
+
+int Engine::serve_stop() {
+  {
+    std::lock_guard<std::mutex> q(srv.qmu);
+    if (!srv.running) return DSM_OK;
+    srv.stopping = true;
+    srv.work_cv.notify_all();
+  }
+  srv.worker.join();
+  std::lock_guard<std::mutex> q(srv.qmu);
+  for (Request &r : srv.pending) srv.tickets[r.id] = Outcome{DSM_ERR_OOM, 0, "serving stopped before admission"};
+  srv.pending.clear();
+  srv.running = false;
+  srv.stopping = false;
+  srv.done_cv.notify_all();
+  return DSM_OK;
+}
+
+int Engine::register_async(const uint32_t *qoff, const uint32_t *qnbr, const uint32_t *qlab, uint32_t nq,
+                           uint64_t *ticket) {
+  Request r;
+  r.kind = kReqRegister;
+  std::string err;
+  if (int rc = plan_query(nq, qoff, qnbr, qlab, r.plan, err)) return fail(rc, err);
+  r.t_submit = std::chrono::steady_clock::now();
+  std::lock_guard<std::mutex> q(srv.qmu);
+  if (!srv.running || srv.stopping) return fail(DSM_ERR_STATE, "the serving loop is not running");
+  r.id = *ticket = srv.next_ticket++;
+  srv.queue.push_back(std::move(r));
+  srv.work_cv.notify_one();
+  return DSM_OK;
+}
+
+int Engine::retire_async(uint32_t qid, uint64_t *ticket) {
+  Request r;
+  r.kind = kReqRetire;
+  r.qid = qid;
+  r.t_submit = std::chrono::steady_clock::now();
+  std::lock_guard<std::mutex> q(srv.qmu);
+  if (!srv.running || srv.stopping) return fail(DSM_ERR_STATE, "the serving loop is not running");
+  r.id = *ticket = srv.next_ticket++;
+  srv.queue.push_back(std::move(r));
+  srv.work_cv.notify_one();
+  return DSM_OK;
+}
+
+int Engine::admission(uint64_t ticket, int64_t timeout_ms, uint32_t *qid) {
+  std::unique_lock<std::mutex> q(srv.qmu);
+  if (ticket == 0 || ticket >= srv.next_ticket) return fail(DSM_ERR_NOT_FOUND, "no such ticket");
+  auto ready = [&] { return srv.tickets.count(ticket) != 0; };
+  if (timeout_ms < 0) srv.done_cv.wait(q, ready);
+  else if (!srv.done_cv.wait_for(q, std::chrono::milliseconds(timeout_ms), ready))
+    return DSM_ERR_TIMEOUT;
+  const Outcome &o = srv.tickets[ticket];
+  if (o.rc) {
+    last_error = o.msg;
+    return o.rc;
+  }
+  *qid = o.qid;
+  return DSM_OK;
+}
+
+// Registrations that wait for memory, first come first served (mu held).
+void Engine::admit_pending() {
+  for (;;) {
+    Request r;
+    {
+      std::lock_guard<std::mutex> q(srv.qmu);
+      if (srv.pending.empty()) return;
+      r = std::move(srv.pending.front());
+      srv.pending.pop_front();
+    }
+    uint32_t qid = 0;
+    bool later = false;
+    const int rc = admit(r.plan, &qid, &later);
+    std::lock_guard<std::mutex> q(srv.qmu);
+    if (rc == DSM_ERR_OOM && later) {  // still does not fit: keep its place
+      srv.pending.push_front(std::move(r));
+      return;
+    }
+    srv.tickets[r.id] = Outcome{rc, qid, rc ? last_error : std::string()};
+    srv.done_cv.notify_all();
+  }
+}
+
+Outcome Engine::handle_control(Request &r) {
+  std::lock_guard<std::mutex> lk(mu);
+  Outcome o;
+  if (r.kind == kReqRetire) {
+    o.rc = retire_locked(r.qid);
+    o.qid = r.qid;
+    if (o.rc) o.msg = last_error;
+    admit_pending();
+    return o;
+  }
+  // a registration queues behind earlier ones still waiting for memory
+  bool behind;
+  {
+    std::lock_guard<std::mutex> q(srv.qmu);
+    behind = !srv.pending.empty();
+  }
+  bool later = true;
+  o.rc = behind ? DSM_ERR_OOM : admit(r.plan, &o.qid, &later);
+  if (behind) later = query_footprint(r.plan) + (bytes_in_use - std::min(bytes_in_use, query_bytes_allocated())) <=
+                      budget;
+  if (o.rc == DSM_ERR_OOM && later) {
+    std::lock_guard<std::mutex> q(srv.qmu);
+    srv.pending.push_back(std::move(r));
+    o.rc = -1;  // no outcome yet
+    return o;
+  }
+  if (o.rc) o.msg = last_error;
+  return o;
+}
+
+void Engine::worker_loop() {
+  cudaSetDevice(device);
+  std::unique_lock<std::mutex> q(srv.qmu);
+  for (;;) {
+    srv.work_cv.wait(q, [&] { return !srv.queue.empty() || srv.stopping; });
+    if (srv.queue.empty()) break;  // stopping, and everything queued was served
+    if (srv.queue.front().kind != kReqBatch) {
+      Request r = std::move(srv.queue.front());
+      srv.queue.pop_front();
+      q.unlock();
+      Outcome o = handle_control(r);
+      q.lock();
+      if (o.rc != -1) srv.tickets[r.id] = o;
+      srv.done_cv.notify_all();
+      continue;
+    }
+    std::vector<Request> reqs;
+    size_t total = 0;
+    while (!srv.queue.empty() && srv.queue.front().kind == kReqBatch &&
+           (reqs.empty() || total + srv.queue.front().ups.size() <= srv.max_merge)) {
+      total += srv.queue.front().ups.size();
+      reqs.push_back(std::move(srv.queue.front()));
+      srv.queue.pop_front();
+    }
+    q.unlock();
+    run_merged(reqs);
+    q.lock();
+    srv.done_cv.notify_all();
+  }
+}
+
+// One device batch for consecutive batch requests; each request gets its own
+// result (its updates' slice of every per-(query, update) array).
+void Engine::run_merged(std::vector<Request> &reqs) {
+  std::vector<dsm_update> all;
+  std::vector<uint32_t> start(reqs.size() + 1, 0);
+  for (size_t k = 0; k < reqs.size(); ++k) {
+    all.insert(all.end(), reqs[k].ups.begin(), reqs[k].ups.end());
+    start[k + 1] = (uint32_t)all.size();
+  }
+  const uint32_t N = (uint32_t)all.size();
+  BatchResult R;
+  int rc;
+  std::string msg;
+  std::chrono::steady_clock::time_point t0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    t0 = std::chrono::steady_clock::now();
+    cudaSetDevice(device);
+    rc = run_batch(all.data(), N, R);
+    if (rc) msg = last_error;
+  }
+  if (rc) {
+    std::lock_guard<std::mutex> q(srv.qmu);
+    for (Request &r : reqs) {
+      srv.failed[r.id] = Outcome{rc, 0, msg};
+      srv.done.insert(r.id);
+    }
+    return;
+  }
+  const uint32_t nql = (uint32_t)R.qids.size();
+  std::vector<std::unique_ptr<BatchResult>> outs;
+  for (size_t k = 0; k < reqs.size(); ++k) {
+    const uint32_t s = start[k], n = start[k + 1] - s;
+    auto o = std::make_unique<BatchResult>();
+    o->id = reqs[k].id;
+    o->n = n;
+    o->qids = R.qids;
+    o->widths = R.widths;
+    o->listed = R.listed;
+    o->signs.assign(R.signs.begin() + s, R.signs.begin() + s + n);
+    o->counts.resize((size_t)nql * n);
+    o->offsets.assign((size_t)nql * n + 1, 0);
+    for (uint32_t ql = 0; ql < nql; ++ql)
+      for (uint32_t i = 0; i < n; ++i) {
+        const size_t src = (size_t)ql * N + s + i, dst = (size_t)ql * n + i;
+        o->counts[dst] = R.counts[src];
+        o->offsets[dst + 1] = o->offsets[dst] + (R.offsets[src + 1] - R.offsets[src]);
+      }
+    if (R.listed) {
+      o->tuples.resize(o->offsets.back());
+      for (uint32_t ql = 0; ql < nql; ++ql) {  // each query's slice is contiguous
+        const size_t a = R.offsets[(size_t)ql * N + s], b = R.offsets[(size_t)ql * N + s + n];
+        std::copy(R.tuples.begin() + a, R.tuples.begin() + b, o->tuples.begin() + o->offsets[(size_t)ql * n]);
+      }
+    }
+    o->device_ms = R.device_ms;
+    o->match_ms = R.match_ms;
+    o->merged_requests = (uint32_t)reqs.size();
+    o->merged_updates = N;
+    outs.push_back(std::move(o));
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  {
+    std::lock_guard<std::mutex> r(rmu);
+    for (size_t k = 0; k < reqs.size(); ++k) {
+      outs[k]->queue_ms = ms_between(reqs[k].t_submit, t0);
+      outs[k]->service_ms = ms_between(t0, t1);
+      outs[k]->total_ms = ms_between(reqs[k].t_submit, t1);
+      results[reqs[k].id] = std::move(outs[k]);
+    }
+  }
+  std::lock_guard<std::mutex> q(srv.qmu);
+  for (Request &r : reqs) srv.done.insert(r.id);
+}
+
+}  // namespace dsm

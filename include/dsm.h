@@ -9,8 +9,9 @@
  * host globals and __constant__ symbols, so one query per process.
  *
  * One engine = one device, one CUDA stream, one data graph, any number of
- * registered queries.  Calls on one engine are serialised internally (a
- * mutex), so the ABI is thread-safe per engine.
+ * registered queries.  Calls on one engine are serialised internally
+ * (mutexes), so the ABI is thread-safe per engine; with the serving loop
+ * running, batches and query changes go through its submission queue.
  */
 #ifndef DSM_H
 #define DSM_H
@@ -57,7 +58,7 @@ const char *dsm_last_error(dsm_engine *e);
 
 /* Options (dsm_engine_set_option). */
 #define DSM_OPT_LIST 1          /* 1: list embeddings (default); 0: counts only */
-#define DSM_OPT_FILTER 2        /* 0: labels only; 1: LDF+NLF; 2: cluster encoding (default) */
+#define DSM_OPT_FILTER 2        /* 0: labels only (default); 1: LDF+NLF; 2: cluster encoding */
 #define DSM_OPT_RESULT_CAP 3    /* initial result capacity in tuples (grows on overflow) */
 #define DSM_OPT_WARPS_PER_SM 4  /* persistent matcher warps per SM (autotuned when 0) */
 #define DSM_OPT_DONATE 5        /* 0 disables work donation between warps */
@@ -66,6 +67,8 @@ const char *dsm_last_error(dsm_engine *e);
 #define DSM_OPT_SORT 8          /* 1: canonically sort each update's tuples (default) */
 #define DSM_OPT_LIST_LIMIT 9    /* bytes of tuples one batch may list; beyond it the batch
                                    returns exact counts only and its view has listed = 0 */
+#define DSM_OPT_MEM_BUDGET 10   /* device memory budget in bytes (>= bytes in use); raising it
+                                   admits queries that waited for memory */
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
 int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
 
@@ -94,6 +97,7 @@ int dsm_graph_info(dsm_engine *e, uint32_t *nv, uint64_t *num_entries, uint64_t 
  * footprint does not fit the engine's memory budget. */
 int dsm_query_register(dsm_engine *e, const uint32_t *q_offsets, const uint32_t *q_nbrs,
                        const uint32_t *q_labels, uint32_t nq, uint32_t *qid);
+/* Ends matching for qid; a later registration may reuse the id. */
 int dsm_query_retire(dsm_engine *e, uint32_t qid);
 /* Matching order for ordered query edge (u, v): order[p] = query vertex at
  * position p; bn_mask[p] = positions < p adjacent to it (OrderCPU's
@@ -119,8 +123,10 @@ int dsm_query_plan(const uint32_t *q_offsets, const uint32_t *q_nbrs, const uint
  * re-upload, re-filter, seeding, the matcher of gpu_match.cu/join.cu) for all
  * registered queries at once.  Updates apply in array order with sequential
  * semantics: an insert's positive matches are taken on the graph after it,
- * a delete's negative matches on the graph before it.  Asynchronous: returns
- * once the batch is queued on the engine stream. */
+ * a delete's negative matches on the graph before it.  Without the serving
+ * loop the call runs the batch to completion (one device batch per call,
+ * the reference's plain form); with it (dsm_serve_start) the call only
+ * queues the batch and returns its id. */
 int dsm_batch_submit(dsm_engine *e, const dsm_update *ups, uint32_t n, uint64_t *batch_id);
 /* Blocks until the batch's results are on the host. */
 int dsm_batch_wait(dsm_engine *e, uint64_t batch_id);
@@ -140,6 +146,48 @@ typedef struct dsm_result_view {
 /* Waits if needed; the view stays valid until dsm_batch_release. */
 int dsm_batch_results(dsm_engine *e, uint64_t batch_id, dsm_result_view *view);
 int dsm_batch_release(dsm_engine *e, uint64_t batch_id);
+
+/* Latency of one submitted batch (host steady clock), available once it is
+ * done and until it is released. */
+typedef struct dsm_batch_timing {
+  double queue_ms;            /* submit -> its device batch started */
+  double service_ms;          /* device batch started -> results readable */
+  double total_ms;            /* submit -> results readable */
+  double device_ms;           /* device time of its device batch (events) */
+  uint32_t merged_requests;   /* submitted batches served by that device batch */
+  uint32_t merged_updates;    /* updates in that device batch */
+} dsm_batch_timing;
+int dsm_batch_timing_get(dsm_engine *e, uint64_t batch_id, dsm_batch_timing *t);
+
+/* ---- serving loop ----------------------------------------------------- */
+/* No counterpart in the reference (its main loop handles one query and one
+ * batch at a time, main.cu:152-347).  dsm_serve_start starts one worker
+ * thread per engine that serves requests in submission order:
+ * dsm_batch_submit then only queues the batch and returns its id; batches
+ * that are queued back to back run as ONE device batch of up to
+ * max_merge_updates updates (0 = 65536), whose per-update results equal
+ * those of running them one by one (each update still sees exactly the
+ * updates before it); registrations and retirements take effect between
+ * device batches, in submission order.  Admission: a query is charged its
+ * device footprint (descriptor, orders, filter bitmaps and encodings); one
+ * that does not fit the memory budget now waits, first come first served,
+ * until retirements free enough, and one that could never fit fails with
+ * DSM_ERR_OOM.  While serving, dsm_query_register and dsm_query_retire queue
+ * their request and block until it took effect.  dsm_serve_stop serves what
+ * is queued, then joins the worker (registrations still waiting for memory
+ * fail with DSM_ERR_OOM).  The device batch limits (listing limit, result
+ * capacity) apply to the merged batch. */
+int dsm_serve_start(dsm_engine *e, uint32_t max_merge_updates);
+int dsm_serve_stop(dsm_engine *e);
+/* Queues a registration; *ticket names it for dsm_query_admission. */
+int dsm_query_register_async(dsm_engine *e, const uint32_t *q_offsets, const uint32_t *q_nbrs,
+                             const uint32_t *q_labels, uint32_t nq, uint64_t *ticket);
+/* Queues a retirement; its ticket's outcome is reported like a registration's. */
+int dsm_query_retire_async(dsm_engine *e, uint32_t qid, uint64_t *ticket);
+/* Waits up to timeout_ms (< 0: no limit) for a ticket's outcome: DSM_OK
+ * (with *qid: the admitted or retired query) once it took effect,
+ * DSM_ERR_TIMEOUT while it still waits, else the request's error. */
+int dsm_query_admission(dsm_engine *e, uint64_t ticket, int64_t timeout_ms, uint32_t *qid);
 
 /* ---- counting without allocating ------------------------------------- */
 /* No counterpart in the reference: an entry point for callers that must not
@@ -194,6 +242,8 @@ typedef struct dsm_stats {
   double last_sort_ms;
   uint64_t device_bytes_in_use;
   uint64_t kernel_launches;  /* engine kernels launched so far */
+  uint64_t query_bytes;      /* device bytes charged to admitted queries */
+  uint64_t live_queries;
 } dsm_stats;
 int dsm_engine_stats(dsm_engine *e, dsm_stats *s);
 

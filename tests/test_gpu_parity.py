@@ -99,6 +99,48 @@ def test_c2_scaled_listing(qi):
     e.close()
 
 
+@pytest.mark.parametrize("k", [0, 1])
+def test_c4_thirty_two_labels(k):
+    """Config 4 shape (R-MAT, 32 uniform labels: the last label slot is in
+    use) at 2^16 vertices; the first two pool queries that carry label 31.
+    Listed, two lognormal-size batches."""
+    w = d.Workload(4, scale_log2=-8, num_batches=2)
+    q = [q for q in w.queries if 31 in q.labels.tolist()][k]
+    e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
+    st = oracle_stream(w.nv, w.labels, w.edges, q)
+    total, checked = run_stream(e, [qid], [st], list(w.batches()), check_graph_every=1, limit=100_000)
+    assert checked >= 64, checked
+    e.close()
+
+
+def test_labels_beyond_the_last_slot():
+    """Data labels 29..34: labels >= 31 share the last slot of the
+    label-major runs, and a query vertex with label 31 must match only data
+    vertices whose label is exactly 31 (about 600 embeddings per query over
+    2500 updates)."""
+    rng = np.random.default_rng(7)
+    nv = 1000
+    labels = rng.integers(29, 35, nv).astype(np.uint32)
+    edges = set()
+    while len(edges) < 20000:
+        a, b = (int(x) for x in rng.integers(0, nv, 2))
+        if a != b:
+            edges.add((min(a, b), max(a, b)))
+    edges = np.array(sorted(edges), np.uint32)
+    keep = np.ones(len(edges), bool)
+    keep[rng.choice(len(edges), 1500, replace=False)] = False
+    init, held = edges[keep], edges[~keep]
+    ups = np.array([[1, a, b, 0] for a, b in held] + [[0, a, b, 0] for a, b in init[:1000]], np.uint32)
+    ups = ups[rng.permutation(len(ups))]
+    for ql in ([31, 31, 30, 29], [31, 29, 31, 31]):
+        q = d.Query.from_edges(ql, [(0, 1), (1, 2), (0, 2), (2, 3)])
+        e, (qid,) = _fresh(nv, labels, init, [q])
+        st = oracle_stream(nv, labels, init, q)
+        total, _ = run_stream(e, [qid], [st], [ups[:1200], ups[1200:]], check_graph_every=1)
+        assert total > 500
+        e.close()
+
+
 def test_listing_limit_downgrades_to_counts():
     w = d.Workload(1, scale_log2=-2)
     b = np.concatenate(list(w.batches())[:400])
