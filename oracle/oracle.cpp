@@ -12,7 +12,12 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <fstream>
 #include <map>
 #include <queue>
@@ -707,6 +712,150 @@ uint64_t match_edge(const Stream &S, uint32_t a, uint32_t b, bool list, std::vec
   return cnt;
 }
 
+// ------------------------------------------------------------------------
+// The same per-update matcher on many host threads: updates still apply one
+// at a time in stream order; inside one update, the seeds' search trees are
+// expanded breadth-first into a frontier of partial embeddings (at least
+// 16 per thread), which the threads then expand depth-first.
+// ------------------------------------------------------------------------
+struct Pool {
+  std::vector<std::thread> th;
+  std::mutex m;
+  std::condition_variable cv, done_cv;
+  std::function<void(int)> job;
+  uint64_t gen = 0;
+  int pending = 0;
+  bool stop = false;
+  explicit Pool(int n) {
+    for (int t = 0; t < n; ++t)
+      th.emplace_back([this, t] {
+        uint64_t seen = 0;
+        for (;;) {
+          std::unique_lock<std::mutex> lk(m);
+          cv.wait(lk, [&] { return stop || gen != seen; });
+          if (stop) return;
+          seen = gen;
+          lk.unlock();
+          job(t);
+          lk.lock();
+          if (--pending == 0) done_cv.notify_all();
+        }
+      });
+  }
+  void run(std::function<void(int)> f) {
+    std::unique_lock<std::mutex> lk(m);
+    job = std::move(f);
+    pending = (int)th.size();
+    ++gen;
+    cv.notify_all();
+    done_cv.wait(lk, [&] { return pending == 0; });
+  }
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> lk(m);
+      stop = true;
+    }
+    cv.notify_all();
+    for (auto &t : th) t.join();
+  }
+};
+
+struct Partial {
+  uint32_t seed;
+  uint32_t depth;
+  std::array<uint32_t, 16> f;
+};
+
+// Children of a partial embedding (one level of enumerate()).
+void expand_one(const Stream &S, const Partial &x, std::vector<Partial> &out) {
+  const Stream::Seed &sd = S.seeds[x.seed];
+  const uint32_t p = x.depth, u = sd.order[p], mask = sd.bn[p];
+  int pivot = -1;
+  for (uint32_t j = 0; j < p; ++j)
+    if (mask & (1u << j))
+      if (pivot < 0 || S.adj[x.f[j]].size() < S.adj[x.f[pivot]].size()) pivot = (int)j;
+  for (uint32_t w : S.adj[x.f[pivot]]) {
+    if (S.labels[w] != S.qlabels[u]) continue;
+    bool ok = true;
+    for (uint32_t j = 0; j < p && ok; ++j)
+      if (x.f[j] == w) ok = false;
+    for (uint32_t j = 0; j < p && ok; ++j)
+      if ((mask & (1u << j)) && (int)j != pivot && !S.has_edge(x.f[j], w)) ok = false;
+    if (!ok) continue;
+    Partial y = x;
+    y.f[p] = w;
+    y.depth = p + 1;
+    out.push_back(y);
+  }
+}
+
+uint64_t match_edge_mt(const Stream &S, uint32_t a, uint32_t b, bool list, std::vector<uint32_t> &out,
+                       Pool &pool, int nt) {
+  std::vector<Partial> front;
+  for (uint32_t k = 0; k < S.seeds.size(); ++k) {
+    const auto &sd = S.seeds[k];
+    if (S.labels[a] != S.qlabels[sd.u] || S.labels[b] != S.qlabels[sd.v]) continue;
+    Partial x;
+    x.seed = k;
+    x.depth = 2;
+    x.f[0] = a;
+    x.f[1] = b;
+    front.push_back(x);
+  }
+  // breadth-first until there is enough work to share (or leaves are reached)
+  uint64_t done_cnt = 0;
+  std::vector<uint32_t> done_tuples;
+  while (!front.empty() && front.size() < (size_t)16 * nt) {
+    std::vector<Partial> next;
+    for (const Partial &x : front) {
+      if (x.depth == S.nq) {
+        ++done_cnt;
+        if (list) {
+          const auto &sd = S.seeds[x.seed];
+          size_t base = done_tuples.size();
+          done_tuples.resize(base + S.nq);
+          for (uint32_t k = 0; k < S.nq; ++k) done_tuples[base + sd.order[k]] = x.f[k];
+        }
+        continue;
+      }
+      expand_one(S, x, next);
+    }
+    front.swap(next);
+  }
+  std::atomic<size_t> next_task{0};
+  std::vector<uint64_t> cnt(nt, 0);
+  std::vector<std::vector<uint32_t>> tup(nt);
+  pool.run([&](int t) {
+    std::vector<uint32_t> f(S.nq);
+    uint64_t bytes = 0;
+    for (size_t i; (i = next_task.fetch_add(1)) < front.size();) {
+      const Partial &x = front[i];
+      std::copy(x.f.begin(), x.f.begin() + x.depth, f.begin());
+      enumerate(S, S.seeds[x.seed], f, x.depth, list, cnt[t], tup[t], bytes);
+    }
+  });
+  uint64_t total = done_cnt;
+  for (int t = 0; t < nt; ++t) total += cnt[t];
+  if (list) {
+    const size_t first = out.size(), w = S.nq;
+    out.insert(out.end(), done_tuples.begin(), done_tuples.end());
+    for (int t = 0; t < nt; ++t) out.insert(out.end(), tup[t].begin(), tup[t].end());
+    const size_t n = (out.size() - first) / w;
+    std::vector<uint32_t> idx(n);
+    for (size_t i = 0; i < n; ++i) idx[i] = (uint32_t)i;
+    const uint32_t *base = out.data() + first;
+    std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+      return std::lexicographical_compare(base + (size_t)x * w, base + (size_t)x * w + w, base + (size_t)y * w,
+                                          base + (size_t)y * w + w);
+    });
+    std::vector<uint32_t> sorted(n * w);
+    for (size_t i = 0; i < n; ++i)
+      std::copy(base + (size_t)idx[i] * w, base + (size_t)idx[i] * w + w, sorted.begin() + i * w);
+    std::copy(sorted.begin(), sorted.end(), out.begin() + first);
+  }
+  return total;
+}
+
 void count_all_rec(const Stream &S, const std::vector<uint32_t> &order,
                    const std::vector<uint32_t> &bn, std::vector<uint32_t> &f, size_t p,
                    uint64_t &cnt) {
@@ -909,6 +1058,56 @@ int orc_stream_apply(orc_stream *h, uint32_t n, const uint32_t *ups, int list) {
   }
   for (uint32_t i = S.complete; i < n; ++i) S.count[i] = 0;
   return S.complete < n ? 1 : 0;
+}
+
+int orc_stream_apply_mt(orc_stream *h, uint32_t n, const uint32_t *ups, int list, int threads) {
+  Stream &S = h->s;
+  if (threads < 1) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  Pool pool(threads);
+  S.sign.assign(n, 0);
+  S.count.assign(n, 0);
+  S.tuples.clear();
+  S.complete = n;
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t op = ups[4 * i], a = ups[4 * i + 1], b = ups[4 * i + 2];
+    if (a >= S.nv || b >= S.nv) return -1;
+    if (a == b) continue;
+    bool present = S.has_edge(a, b);
+    auto &la = S.adj[a], &lb = S.adj[b];
+    if (op == 1) {
+      if (present) continue;
+      la.insert(std::lower_bound(la.begin(), la.end(), b), b);
+      lb.insert(std::lower_bound(lb.begin(), lb.end(), a), a);
+      S.sign[i] = 1;
+      S.count[i] = match_edge_mt(S, a, b, list != 0, S.tuples, pool, threads);
+    } else {
+      if (!present) continue;
+      S.sign[i] = -1;
+      S.count[i] = match_edge_mt(S, a, b, list != 0, S.tuples, pool, threads);
+      la.erase(std::lower_bound(la.begin(), la.end(), b));
+      lb.erase(std::lower_bound(lb.begin(), lb.end(), a));
+    }
+  }
+  return 0;
+}
+
+int orc_stream_apply_graph(orc_stream *h, uint32_t n, const uint32_t *ups) {
+  Stream &S = h->s;
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t op = ups[4 * i], a = ups[4 * i + 1], b = ups[4 * i + 2];
+    if (a >= S.nv || b >= S.nv) return -1;
+    if (a == b) continue;
+    bool present = S.has_edge(a, b);
+    auto &la = S.adj[a], &lb = S.adj[b];
+    if (op == 1 && !present) {
+      la.insert(std::lower_bound(la.begin(), la.end(), b), b);
+      lb.insert(std::lower_bound(lb.begin(), lb.end(), a), a);
+    } else if (op == 0 && present) {
+      la.erase(std::lower_bound(la.begin(), la.end(), b));
+      lb.erase(std::lower_bound(lb.begin(), lb.end(), a));
+    }
+  }
+  return 0;
 }
 
 void orc_stream_set_budget(orc_stream *h, uint64_t bytes) { h->s.work_budget = bytes; }

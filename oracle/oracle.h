@@ -102,6 +102,12 @@ int orc_stream_apply(orc_stream *s, uint32_t n, const uint32_t *updates, int lis
  * first orc_stream_complete() updates have full results, the rest have
  * count 0, and apply returns 1.  Lets tests afford explosive updates. */
 void orc_stream_set_budget(orc_stream *s, uint64_t bytes);
+/* orc_stream_apply on `threads` host threads (< 1: all cores): the same
+ * results; updates apply in order, each update's search is shared among the
+ * threads.  No work budget. */
+int orc_stream_apply_mt(orc_stream *s, uint32_t n, const uint32_t *updates, int list, int threads);
+/* Applies the updates to the graph only (no matching). */
+int orc_stream_apply_graph(orc_stream *s, uint32_t n, const uint32_t *updates);
 uint32_t orc_stream_complete(const orc_stream *s);
 int8_t orc_stream_sign(const orc_stream *s, uint32_t i);
 uint64_t orc_stream_count(const orc_stream *s, uint32_t i);

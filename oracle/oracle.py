@@ -42,6 +42,8 @@ _sig("orc_cluster_filter", C.c_int, C.c_uint32, u32p, u32p, u32p, C.c_uint32, u3
 _sig("orc_stream_new", C.c_int, C.c_uint32, u32p, C.c_uint64, u32p, C.c_uint32, u32p, u32p, u32p, C.POINTER(P))
 _sig("orc_stream_free", None, P)
 _sig("orc_stream_apply", C.c_int, P, C.c_uint32, u32p, C.c_int)
+_sig("orc_stream_apply_mt", C.c_int, P, C.c_uint32, u32p, C.c_int, C.c_int)
+_sig("orc_stream_apply_graph", C.c_int, P, C.c_uint32, u32p)
 _sig("orc_stream_set_budget", None, P, C.c_uint64)
 _sig("orc_stream_complete", C.c_uint32, P)
 _sig("orc_stream_sign", C.c_int8, P, C.c_uint32)
@@ -143,13 +145,18 @@ class Stream:
             lib.orc_stream_free(self._h)
             self._h = None
 
-    def apply(self, updates, listed=True):
-        """Returns (signs[n], counts[n], list of (count, nq) arrays or None)."""
+    def apply(self, updates, listed=True, threads=0):
+        """Returns (signs[n], counts[n], list of (count, nq) arrays or None).
+        threads > 0: the multi-threaded matcher on that many host threads
+        (threads < 0: all cores); no work budget."""
         u = _u32(updates).reshape(-1)
         n = len(u) // 4
         if n == 0:
             return np.zeros(0, np.int8), np.zeros(0, np.uint64), []
-        rc = lib.orc_stream_apply(self._h, n, u, int(listed))
+        if threads:
+            rc = lib.orc_stream_apply_mt(self._h, n, u, int(listed), max(threads, 0))
+        else:
+            rc = lib.orc_stream_apply(self._h, n, u, int(listed))
         if rc not in (0, 1):
             raise ValueError("oracle apply failed")
         # with a work budget, only the first `complete` updates have results
@@ -166,6 +173,12 @@ class Stream:
             out.append(flat[pos:pos + int(c)])
             pos += int(c)
         return signs, counts, out
+
+    def apply_graph(self, updates):
+        """Applies the updates to the graph without matching."""
+        u = _u32(updates).reshape(-1)
+        if len(u) and lib.orc_stream_apply_graph(self._h, len(u) // 4, u):
+            raise ValueError("oracle apply failed")
 
     def set_budget(self, nbytes):
         """Work budget (algorithmic bytes) of each later apply call."""

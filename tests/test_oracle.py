@@ -132,3 +132,29 @@ def test_parser_rejects_malformed(tmp_path):
     p.write_text("t 2 1\nv 1 0 1\nv 0 0 1\ne 0 1\n")
     with pytest.raises(ValueError):
         orc.parse(str(p), True)
+
+
+@pytest.mark.parametrize("qi", range(len(QUERIES)))
+def test_multithreaded_matcher_equals_sequential(qi):
+    """The all-cores matcher (the CPU baseline) gives the sequential one's
+    signs, counts and sorted tuples; apply_graph reaches the same graph."""
+    rng = np.random.default_rng(11 + qi)
+    labels, edges = _random_graph(rng, 60, 400, 2)
+    ql, qe = QUERIES[qi]
+    qoff, qnb = _csr(len(ql), qe)
+    ups = []
+    for _ in range(300):
+        a, b = (int(x) for x in rng.integers(0, 60, 2))
+        ups.append([int(rng.integers(0, 2)), a, b, 0])
+    ups = np.array(ups, np.uint32)
+    one = orc.Stream(60, labels, edges, np.array(ql, np.uint32), qoff, qnb)
+    many = orc.Stream(60, labels, edges, np.array(ql, np.uint32), qoff, qnb)
+    graph = orc.Stream(60, labels, edges, np.array(ql, np.uint32), qoff, qnb)
+    s1, c1, t1 = one.apply(ups)
+    s2, c2, t2 = many.apply(ups, threads=4)
+    graph.apply_graph(ups)
+    assert c1.sum() > 0
+    assert np.array_equal(s1, s2) and np.array_equal(c1, c2)
+    assert all(np.array_equal(x, y) for x, y in zip(t1, t2))
+    for a, b in zip(one.export(), graph.export()):
+        assert np.array_equal(a, b)
