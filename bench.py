@@ -117,6 +117,8 @@ def run_ours(args, rank, world):
         e = d.Engine(dev)
         e.set_option(d.OPT_LIST, args.list)
         e.set_option(d.OPT_FILTER, args.filter)
+        if args.autotune and args.warmup > 0:  # the first warm-up batch picks the launch setting
+            e.set_option(d.OPT_AUTOTUNE, 1)
         e.load_graph_edges(w.nv, w.labels, w.edges)
         return e, [e.register(q) for q in qs]
 
@@ -206,7 +208,9 @@ def run_ours(args, rank, world):
         "data": "synthetic (seeded Chung-Lu graph, random-walk queries, generated update stream)",
         "config": {"workload": f"config2: Chung-Lu gamma=2.1, |V|=2^{20 + args.scale}, |E|=2^{24 + args.scale}, "
                                "16 Zipf(1.2) labels, three 8-vertex queries, batches of 4096 (50/50)",
-                   "form": args.form, "listing": bool(args.list), "filter": args.filter, "parallelism": f"replicas x{world}",
+                   "form": args.form, "listing": bool(args.list), "filter": args.filter,
+                   "tuned": {k: engines[0][0].get_option(getattr(d, "OPT_" + k.upper()))
+                             for k in ("warps_per_sm", "split_min", "donate_depth")}, "parallelism": f"replicas x{world}",
                    "l2": "256 MiB buffer written between timed batches"},
         "updates_per_sec": upd / (dev_ms / 1e3) if dev_ms > 0 else 0.0,
         "matches": matches,
@@ -426,6 +430,7 @@ def main():
     ap.add_argument("--list", type=int, default=0)
     ap.add_argument("--filter", type=int, default=0, help="candidate filter: 0 none, 1 LDF+NLF, 2 cluster encoding")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--autotune", type=int, default=1, help="1: tune the matcher launch on the first warm-up batch")
     ap.add_argument("--scale", type=int, default=0, help="log2 shrink of the graph (0 = config size)")
     ap.add_argument("--ref-step-s", type=float, default=5.0, help="CPU arm: seconds of matching per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -80,6 +80,15 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
       if (value <= 0) return E.fail(DSM_ERR_ARG, "listing limit must be positive");
       E.list_limit_bytes = (uint64_t)value;
       return DSM_OK;
+    case DSM_OPT_SPLIT_MIN:
+      if (value != 0 && (value < 64 || value > (1 << 24))) return E.fail(DSM_ERR_ARG, "split threshold 0 or 64..2^24");
+      E.split_min = (uint32_t)value;
+      return DSM_OK;
+    case DSM_OPT_DONATE_DEPTH:
+      if (value < 0 || value > 4) return E.fail(DSM_ERR_ARG, "donation depth 0..4");
+      E.donate_depth = (uint32_t)value;
+      return DSM_OK;
+    case DSM_OPT_AUTOTUNE: E.tune_next = value != 0; return DSM_OK;
     case DSM_OPT_MEM_BUDGET:
       if (value <= 0 || (uint64_t)value < E.bytes_in_use)
         return E.fail(DSM_ERR_ARG, "budget must cover the bytes in use");
@@ -105,6 +114,9 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_SORT: *value = E.sort_results; return DSM_OK;
     case DSM_OPT_LIST_LIMIT: *value = (int64_t)E.list_limit_bytes; return DSM_OK;
     case DSM_OPT_MEM_BUDGET: *value = (int64_t)E.budget; return DSM_OK;
+    case DSM_OPT_SPLIT_MIN: *value = E.split_min; return DSM_OK;
+    case DSM_OPT_DONATE_DEPTH: *value = E.donate_depth; return DSM_OK;
+    case DSM_OPT_AUTOTUNE: *value = E.tune_next ? 1 : 0; return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");
 }

@@ -649,7 +649,13 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   ma.list = list_mode;
   ma.donate = donate;
   ma.timeout_cycles = (long long)timeout_ms * (long long)clock_khz;
-  const int blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
+  ma.split_min = split_min;
+  ma.donate_depth = donate_depth;
+  int blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
+  if (tune_next && nq_live) {
+    tune_next = false;
+    if ((rc = autotune(ma, seed_cap, nseg, blocks))) return rc;
+  }
   Sched sc;
   int listed = list_mode;  // may drop to counts only for this batch
   int match_rc = DSM_OK;   // a matcher failure still lets the batch's graph updates finish
@@ -798,6 +804,77 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   R.alg_bytes = sc.alg_bytes;
   R.matches = sc.out_count.v;
   return DSM_OK;
+}
+
+// Autotuner: the matcher's result does not depend on its launch shape or on
+// how work is donated, so the batch's own matcher launch is repeated on the
+// same union graph (counts only) for each candidate -- resident blocks per SM
+// x range-split threshold x donation depth -- timed with events, and the
+// fastest becomes the engine's setting.  The first candidate runs twice and
+// its first run is not counted (it warms L2 for all).  Warps per task (1),
+// stack depth (the 16 lane-held levels) and the intersection tile (32
+// entries, one per lane) are fixed by the kernel's design.
+int Engine::autotune(MatchArgs &ma, unsigned long long seed_cap, size_t nseg, int &blocks) {
+  Sched *hs = (Sched *)h_sched.ptr;
+  CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (hs->error) return DSM_OK;  // the real launch reports it
+  const unsigned long long nseeds = hs->nseeds;
+  struct Cand {
+    int bps;
+    uint32_t split, dd;
+  };
+  std::vector<Cand> cands;
+  for (int bps = std::max(1, match_blocks_per_sm - 2); bps <= match_blocks_per_sm; ++bps)
+    for (uint32_t split : {64u, 128u, 512u})
+      for (uint32_t dd : {1u, 2u}) cands.push_back({bps, split, dd});
+  auto rearm = [&]() -> int {
+    std::memset(hs, 0, sizeof(Sched));
+    hs->nseeds = nseeds;
+    CK(cudaMemcpyAsync(d_sched.ptr, hs, sizeof(Sched), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
+    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream);
+    ++stats.kernel_launches;
+    CK(cudaStreamSynchronize(stream));  // hs is read by the copy
+    return DSM_OK;
+  };
+  MatchArgs t = ma;
+  t.list = 0;
+  t.cap = 0;
+  float best = 1e30f;
+  Cand bc{blocks / std::max(num_sms, 1), ma.split_min, ma.donate_depth};
+  cudaEvent_t e0 = ev_pool[2], e1 = ev_pool[3];
+  for (int k = -1; k < (int)cands.size(); ++k) {
+    const Cand &c = cands[std::max(k, 0)];
+    if (int rc = rearm()) return rc;
+    t.split_min = c.split;
+    t.donate_depth = c.dd;
+    CK(cudaEventRecord(e0, stream));
+    launch_match(t, num_sms * c.bps, stream);
+    ++stats.kernel_launches;
+    CK(cudaEventRecord(e1, stream));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (hs->error) break;  // keep the current setting
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    stats.tune_runs++;
+    if (k >= 0 && ms < best) {
+      best = ms;
+      bc = c;
+    }
+  }
+  if (best < 1e30f) {
+    warps_per_sm = bc.bps * 8;
+    split_min = bc.split;
+    donate_depth = bc.dd;
+    stats.tune_best_ms = best;
+  }
+  ma.split_min = split_min;
+  ma.donate_depth = donate_depth;
+  blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
+  return rearm();  // the batch's real launch starts from scratch
 }
 
 // Uploads the filter's descriptor and op list of query `id` and sizes its

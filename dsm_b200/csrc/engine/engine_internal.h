@@ -19,6 +19,7 @@
 #include "../../../include/dsm.h"
 #include "../host/query_plan.h"
 #include "common.cuh"
+#include "kernels.cuh"
 
 namespace dsm {
 
@@ -114,6 +115,8 @@ struct Engine {
   int64_t timeout_ms = 5000;
   int label_quirk = 0;
   int sort_results = 1;
+  uint32_t split_min = 0, donate_depth = 0;  // donation granularity (0 = kernel default)
+  bool tune_next = false;                    // autotune on the next batch
   bool filter_timed = false;  // the filter events of this batch were recorded
   uint64_t result_cap = 1 << 20;
   uint32_t job_ring = 1 << 19;  // job slots of the matcher's donation ring
@@ -175,6 +178,7 @@ struct Engine {
   int query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);
 
   int check_updates(const dsm_update *ups, uint32_t n);
+  int autotune(MatchArgs &ma, unsigned long long seed_cap, size_t nseg, int &blocks);
   int submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id);
   int run_batch(const dsm_update *ups, uint32_t n, BatchResult &R);
   int wait_batch(uint64_t id);

@@ -78,6 +78,11 @@ struct MatchArgs {
   int list;
   int donate;
   long long timeout_cycles;
+  // donation granularity (0 = default): a remaining pivot range is split
+  // when it holds at least split_min entries (>= 64); pending candidates are
+  // donated when at least donate_depth levels lie below them (1..4)
+  uint32_t split_min;
+  uint32_t donate_depth;
 };
 // Arms a matcher launch: outstanding = seeds, every ring slot free for its
 // first position.

@@ -300,6 +300,8 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
         if (__shfl_sync(kFull, err, 0)) break;
       }
       if (P.donate && (ticks & 7) == 0) {
+        const uint32_t split_min = P.split_min > 64 ? P.split_min : (P.split_min ? 64u : 128u);
+        const uint32_t dd = P.donate_depth ? min(P.donate_depth, 4u) : 2u;
         unsigned long long h = 0;
         if (lane == 0) {
           unsigned long long pc = ld_volatile(P.sc->pop_cnt.v), pu = ld_volatile(P.sc->push_cnt.v);
@@ -308,14 +310,15 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
         h = __shfl_sync(kFull, h, 0);
         if (h > 0) {
           // shallowest level with a substantial piece of work: pending
-          // candidates with two or more levels below them, or >= 4 chunks
+          // candidates with dd or more levels below them, or a remaining
+          // range of split_min entries or more
           bool has = lane >= depth && lane <= L &&
-                     ((lv_mask != 0 && lane + 2 < nq) || lv_end >= lv_pos + 128);
+                     ((lv_mask != 0 && lane + dd < nq) || lv_end >= lv_pos + split_min);
           uint32_t hm = __ballot_sync(kFull, has);
           if (hm) {
             const uint32_t p = __ffs(hm) - 1;
             const uint32_t pm0 = __shfl_sync(kFull, lv_mask, p);
-            const uint32_t pm = (p + 2 < nq) ? pm0 : 0u;
+            const uint32_t pm = (p + dd < nq) ? pm0 : 0u;
             uint32_t k, dmask = 0, rmid = 0, rend = 0;
             if (pm) {
               k = min((uint32_t)__popc(pm), (uint32_t)min(h, 32ull));

@@ -60,7 +60,7 @@ const char *dsm_last_error(dsm_engine *e);
 #define DSM_OPT_LIST 1          /* 1: list embeddings (default); 0: counts only */
 #define DSM_OPT_FILTER 2        /* 0: labels only (default); 1: LDF+NLF; 2: cluster encoding */
 #define DSM_OPT_RESULT_CAP 3    /* initial result capacity in tuples (grows on overflow) */
-#define DSM_OPT_WARPS_PER_SM 4  /* persistent matcher warps per SM (autotuned when 0) */
+#define DSM_OPT_WARPS_PER_SM 4  /* persistent matcher warps per SM (0: as many as fit) */
 #define DSM_OPT_DONATE 5        /* 0 disables work donation between warps */
 #define DSM_OPT_TIMEOUT_MS 6    /* bound on every device-side wait (default 5000) */
 #define DSM_OPT_LABEL_QUIRK 7   /* 1: an insert relabels both endpoints (cpuGraph.cpp:564) */
@@ -69,6 +69,16 @@ const char *dsm_last_error(dsm_engine *e);
                                    returns exact counts only and its view has listed = 0 */
 #define DSM_OPT_MEM_BUDGET 10   /* device memory budget in bytes (>= bytes in use); raising it
                                    admits queries that waited for memory */
+#define DSM_OPT_SPLIT_MIN 11    /* work donation: split a remaining pivot range of at least
+                                   this many entries (0 = default 128; else >= 64) */
+#define DSM_OPT_DONATE_DEPTH 12 /* work donation: hand out pending candidates with at least
+                                   this many levels below them (0 = default 2; 1..4) */
+#define DSM_OPT_AUTOTUNE 13     /* 1: the next batch times its matcher launch under each
+                                   candidate setting (resident blocks per SM x split
+                                   threshold x donation depth) on its own union graph and
+                                   keeps the fastest in DSM_OPT_WARPS_PER_SM /
+                                   DSM_OPT_SPLIT_MIN / DSM_OPT_DONATE_DEPTH; its results
+                                   are those of any setting.  Reads 1 until that batch ran. */
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
 int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
 
@@ -244,6 +254,8 @@ typedef struct dsm_stats {
   uint64_t kernel_launches;  /* engine kernels launched so far */
   uint64_t query_bytes;      /* device bytes charged to admitted queries */
   uint64_t live_queries;
+  uint64_t tune_runs;        /* matcher launches timed by the autotuner */
+  double tune_best_ms;       /* the fastest of them (last tuning) */
 } dsm_stats;
 int dsm_engine_stats(dsm_engine *e, dsm_stats *s);
 

@@ -141,6 +141,26 @@ def test_labels_beyond_the_last_slot():
         e.close()
 
 
+def test_autotuned_batch_equals_oracle():
+    """DSM_OPT_AUTOTUNE: the first batch times every candidate launch setting
+    on its own union graph and keeps the fastest; its results and the next
+    batch's (run with the tuned setting) equal the oracle's."""
+    w = d.Workload(2, scale_log2=-6, num_batches=2)
+    q = w.queries[2]
+    e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q], OPT_LIST=0, OPT_AUTOTUNE=1)
+    st = oracle_stream(w.nv, w.labels, w.edges, q)
+    total, checked = run_stream(e, [qid], [st], list(w.batches()), check_graph_every=1, listed=False,
+                                limit=150_000)
+    assert checked >= 1024
+    s = e.stats()
+    assert s["tune_runs"] >= 2 and s["tune_best_ms"] > 0
+    assert e.get_option(d.OPT_AUTOTUNE) == 0
+    assert e.get_option(d.OPT_SPLIT_MIN) in (64, 128, 512)
+    assert e.get_option(d.OPT_DONATE_DEPTH) in (1, 2)
+    assert e.get_option(d.OPT_WARPS_PER_SM) % 8 == 0
+    e.close()
+
+
 def test_listing_limit_downgrades_to_counts():
     w = d.Workload(1, scale_log2=-2)
     b = np.concatenate(list(w.batches())[:400])
