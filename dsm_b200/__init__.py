@@ -19,7 +19,7 @@ ERR = {1: "PARSE", 2: "OOM", 3: "OVERFLOW", 4: "TIMEOUT", 5: "LIMIT", 6: "ARG", 
        9: "NOT_FOUND"}
 
 OPT_LIST, OPT_FILTER, OPT_RESULT_CAP, OPT_WARPS_PER_SM, OPT_DONATE, OPT_TIMEOUT_MS, OPT_LABEL_QUIRK, OPT_SORT, \
-    OPT_LIST_LIMIT, OPT_MEM_BUDGET, OPT_SPLIT_MIN, OPT_DONATE_DEPTH, OPT_AUTOTUNE = range(1, 14)
+    OPT_LIST_LIMIT, OPT_MEM_BUDGET, OPT_SPLIT_MIN, OPT_DONATE_DEPTH, OPT_AUTOTUNE, OPT_GRAPH = range(1, 15)
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is not built; run `python dsm_b200/build.py`")
@@ -46,7 +46,7 @@ class Stats(C.Structure):
                [(n, C.c_double) for n in ("last_batch_ms", "last_match_ms", "last_filter_ms", "last_update_ms",
                                           "last_sort_ms")] + [(n, C.c_uint64) for n in (
                    "device_bytes_in_use", "kernel_launches", "query_bytes", "live_queries", "tune_runs")] + \
-               [("tune_best_ms", C.c_double)]
+               [("tune_best_ms", C.c_double), ("graph_launches", C.c_uint64), ("graph_instantiations", C.c_uint64)]
 
 
 class BatchTiming(C.Structure):

@@ -89,6 +89,7 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
       E.donate_depth = (uint32_t)value;
       return DSM_OK;
     case DSM_OPT_AUTOTUNE: E.tune_next = value != 0; return DSM_OK;
+    case DSM_OPT_GRAPH: E.use_graph = value ? 1 : 0; return DSM_OK;
     case DSM_OPT_MEM_BUDGET:
       if (value <= 0 || (uint64_t)value < E.bytes_in_use)
         return E.fail(DSM_ERR_ARG, "budget must cover the bytes in use");
@@ -117,6 +118,7 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_SPLIT_MIN: *value = E.split_min; return DSM_OK;
     case DSM_OPT_DONATE_DEPTH: *value = E.donate_depth; return DSM_OK;
     case DSM_OPT_AUTOTUNE: *value = E.tune_next ? 1 : 0; return DSM_OK;
+    case DSM_OPT_GRAPH: *value = E.use_graph; return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");
 }

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -105,6 +106,8 @@ Engine::~Engine() {
   serve_stop();
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
+  for (auto &x : gexec)
+    if (x) cudaGraphExecDestroy(x);
   for (DevBuf *b : all_dev_bufs()) dfree(*b);
   for (HostBuf *b : {&h_stage, &h_sched, &h_segcnt, &h_vtp, &h_out_seg, &h_out_tup})
     if (b->ptr) cudaFreeHost(b->ptr);
@@ -594,20 +597,13 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   R.host_prep_ms = std::chrono::duration<double, std::milli>(t_host1 - t_host0).count();
 
   cudaEvent_t ev0 = ev_pool[0], ev_upd = ev_pool[1], ev_m0 = ev_pool[2], ev_m1 = ev_pool[3], ev_end = ev_pool[4];
-  CK(cudaEventRecord(ev0, stream));
-  if (n) CK(cudaMemcpyAsync(d_upd.ptr, st + o_up, up_bytes, cudaMemcpyHostToDevice, stream));
-  if (m) {
-    CK(cudaMemcpyAsync(d_bkey.ptr, st + o_bk, bk_bytes, cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(d_bidx.ptr, st + o_bi, bi_bytes, cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(d_dkey.ptr, st + o_dk, dk_bytes, cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(d_dhead.ptr, st + o_dh, dh_bytes, cudaMemcpyHostToDevice, stream));
-  }
-  CK(cudaMemsetAsync(d_vtp.ptr, 0xFF, nn * 4, stream));
-  CK(cudaMemsetAsync(d_sched.ptr, 0, sizeof(Sched), stream));
-  CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
-  CK(cudaMemsetAsync(d_misc.ptr, 0, 256, stream));
+  // what allocates, synchronises or copies pageable memory runs before the
+  // device segments, so that each segment can be captured into a CUDA graph
   if (qd_dirty)
     if ((rc = upload_qd())) return rc;
+  if ((rc = prepare_filters())) return rc;
+  if ((rc = halloc(h_segcnt, nseg * 8)) || (rc = halloc(h_vtp, nn * 4))) return rc;
+  unsigned int *err_host = (unsigned int *)((char *)h_sched.ptr + sizeof(Sched));  // pinned, 16 bytes
 
   DevGraph g = dev_graph();
   unsigned int *d_err = (unsigned int *)d_misc.ptr;
@@ -615,23 +611,12 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   EdgeStateArgs es{g, (const uint4 *)d_upd.ptr, (const unsigned long long *)d_bkey.ptr,
                    (const uint32_t *)d_bidx.ptr, m, n, (uint32_t *)d_binfo.ptr, (uint8_t *)d_gflag.ptr,
                    (uint32_t *)d_vtp.ptr};
-  launch_edge_state(es, stream);
-  stats.kernel_launches += (m > 0) + (ngroups > 0) + (nq_live > 0 && n > 0) + 1;  // + seeds, sched init
   AdjUpdateArgs au{g, (const unsigned long long *)d_dkey.ptr, (const uint32_t *)d_dhead.ptr, ngroups,
                    (const unsigned long long *)d_bkey.ptr, (const uint8_t *)d_gflag.ptr, m,
                    (uint32_t *)d_dsel.ptr, d_err, d_reloc};
-  launch_adj_insert(au, stream);
-  CK(cudaEventRecord(ev_upd, stream));
-
-  // filters (per query, on the union graph)
-  if ((rc = run_filters())) return rc;
-
   SeedArgs sa{g, (const uint4 *)d_upd.ptr, (const uint32_t *)d_vtp.ptr, n, (const uint32_t *)d_pair_off.ptr,
               (const uint32_t *)d_pair_ent.ptr, (const QDev *)d_qd.ptr, (const OrderRec *)d_orders.ptr,
               (uint4 *)d_seeds.ptr, seed_cap, (Sched *)d_sched.ptr};
-  if (nq_live) launch_seeds(sa, stream);
-  launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream);
-
   MatchArgs ma;
   ma.g = g;
   ma.bt = DevBatchEdges{(const unsigned long long *)d_bkey.ptr, (const uint32_t *)d_binfo.ptr, m};
@@ -652,27 +637,71 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   ma.split_min = split_min;
   ma.donate_depth = donate_depth;
   int blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
-  if (tune_next && nq_live) {
-    tune_next = false;
-    if ((rc = autotune(ma, seed_cap, nseg, blocks))) return rc;
-  }
-  Sched sc;
-  int listed = list_mode;  // may drop to counts only for this batch
-  int match_rc = DSM_OK;   // a matcher failure still lets the batch's graph updates finish
-  for (int attempt = 0;; ++attempt) {
+  auto set_out = [&]() {
     ma.out_seg = (uint32_t *)d_out_seg.ptr;
     ma.out_tup = (uint32_t *)d_out_tup.ptr;
     ma.cap = list_mode ? d_out_seg.bytes / 4 : 0;
     if (list_mode) ma.cap = std::min<unsigned long long>(ma.cap, d_out_tup.bytes / 4 / ma.W);
-    CK(cudaEventRecord(ev_m0, stream));
-    if (nq_live) {
-      launch_match(ma, blocks, stream);
-      ++stats.kernel_launches;
+  };
+  // segment A: uploads, edge state, union insert, filters, seeds, arming
+  auto seg_a = [&]() -> int {
+    if (int r = rec(ev0)) return r;
+    if (n) CK(cudaMemcpyAsync(d_upd.ptr, st + o_up, up_bytes, cudaMemcpyHostToDevice, stream));
+    if (m) {
+      CK(cudaMemcpyAsync(d_bkey.ptr, st + o_bk, bk_bytes, cudaMemcpyHostToDevice, stream));
+      CK(cudaMemcpyAsync(d_bidx.ptr, st + o_bi, bi_bytes, cudaMemcpyHostToDevice, stream));
+      CK(cudaMemcpyAsync(d_dkey.ptr, st + o_dk, dk_bytes, cudaMemcpyHostToDevice, stream));
+      CK(cudaMemcpyAsync(d_dhead.ptr, st + o_dh, dh_bytes, cudaMemcpyHostToDevice, stream));
     }
-    CK(cudaEventRecord(ev_m1, stream));
+    CK(cudaMemsetAsync(d_vtp.ptr, 0xFF, nn * 4, stream));
+    CK(cudaMemsetAsync(d_sched.ptr, 0, sizeof(Sched), stream));
+    CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
+    CK(cudaMemsetAsync(d_misc.ptr, 0, 256, stream));
+    launch_edge_state(es, stream);
+    launch_adj_insert(au, stream);
+    if (int r = rec(ev_upd)) return r;
+    if (int r = launch_filters()) return r;  // per query, on the union graph
+    if (nq_live) launch_seeds(sa, stream);
+    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream);
+    return DSM_OK;
+  };
+  // the matcher launch and the read-back of its scheduler state
+  auto match_launch = [&]() -> int {
+    set_out();
+    if (int r = rec(ev_m0)) return r;
+    if (nq_live) launch_match(ma, blocks, stream);
+    if (int r = rec(ev_m1)) return r;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_sched.ptr, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
+    return DSM_OK;
+  };
+  stats.kernel_launches += (m > 0) + (ngroups > 0) + (nq_live > 0 && n > 0) + 1 + (nq_live > 0);
+  const bool tuning = tune_next && nq_live;
+  const bool graphed = use_graph && !tuning;  // a tuning batch runs eagerly
+  if (graphed) {
+    if ((rc = run_segment(0, [&]() -> int {
+          int r = seg_a();
+          return r ? r : match_launch();
+        })))
+      return rc;
+  } else {
+    if ((rc = seg_a())) return rc;
+    if (tuning) {
+      tune_next = false;
+      if ((rc = autotune(ma, seed_cap, nseg, blocks))) return rc;
+    }
+    if ((rc = match_launch())) return rc;
+  }
+  CK(cudaStreamSynchronize(stream));
+  Sched sc;
+  int listed = list_mode;  // may drop to counts only for this batch
+  int match_rc = DSM_OK;   // a matcher failure still lets the batch's graph updates finish
+  for (int attempt = 0;; ++attempt) {
+    if (attempt > 0) {  // a rerun after the result table grew (eager)
+      if ((rc = match_launch())) return rc;
+      ++stats.kernel_launches;
+      CK(cudaStreamSynchronize(stream));
+    }
     std::memcpy(&sc, h_sched.ptr, sizeof(Sched));
     if (sc.error & kErrTimeout) {
       match_rc = fail(DSM_ERR_TIMEOUT, "matcher: a bounded wait gave up");
@@ -707,31 +736,34 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
     ++stats.kernel_launches;
     CK(cudaStreamSynchronize(stream));
   }
-  unsigned int err_host[4] = {0, 0, 0, 0};
   unsigned long long reloc = 0;
-  // ---- deletions, marks, results
-  launch_adj_delete(au, stream);
-  launch_clear_touch(g, (const uint4 *)d_upd.ptr, n, stream);
-  stats.kernel_launches += (ngroups > 0) + (n > 0);
-  CK(cudaEventRecord(ev_end, stream));
-  size_t cnt = (listed && match_rc == DSM_OK) ? (size_t)sc.out_count.v : 0;
-  if ((rc = halloc(h_segcnt, nseg * 8)) || (rc = halloc(h_vtp, nn * 4))) return rc;
-  if (cnt) {
+  // ---- segment B: deletions, marks, results
+  const size_t cnt = (listed && match_rc == DSM_OK) ? (size_t)sc.out_count.v : 0;
+  if (cnt)
     if ((rc = halloc(h_out_seg, cnt * 4)) || (rc = halloc(h_out_tup, cnt * ma.W * 4))) return rc;
-    CK(cudaMemcpyAsync(h_out_seg.ptr, d_out_seg.ptr, cnt * 4, cudaMemcpyDeviceToHost, stream));
-    CK(cudaMemcpyAsync(h_out_tup.ptr, d_out_tup.ptr, cnt * ma.W * 4, cudaMemcpyDeviceToHost, stream));
-  }
-  CK(cudaMemcpyAsync(h_segcnt.ptr, d_segcnt.ptr, nseg * 8, cudaMemcpyDeviceToHost, stream));
-  CK(cudaMemcpyAsync(h_vtp.ptr, d_vtp.ptr, nn * 4, cudaMemcpyDeviceToHost, stream));
-  CK(cudaMemcpyAsync(err_host, d_misc.ptr, 16, cudaMemcpyDeviceToHost, stream));
+  auto seg_b = [&]() -> int {
+    launch_adj_delete(au, stream);
+    launch_clear_touch(g, (const uint4 *)d_upd.ptr, n, stream);
+    if (int r = rec(ev_end)) return r;
+    if (cnt) {
+      CK(cudaMemcpyAsync(h_out_seg.ptr, d_out_seg.ptr, cnt * 4, cudaMemcpyDeviceToHost, stream));
+      CK(cudaMemcpyAsync(h_out_tup.ptr, d_out_tup.ptr, cnt * ma.W * 4, cudaMemcpyDeviceToHost, stream));
+    }
+    CK(cudaMemcpyAsync(h_segcnt.ptr, d_segcnt.ptr, nseg * 8, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(h_vtp.ptr, d_vtp.ptr, nn * 4, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(err_host, d_misc.ptr, 16, cudaMemcpyDeviceToHost, stream));
+    return DSM_OK;
+  };
+  stats.kernel_launches += (ngroups > 0) + (n > 0);
+  if ((rc = graphed ? run_segment(1, seg_b) : seg_b())) return rc;
   CK(cudaStreamSynchronize(stream));
   std::memcpy(&reloc, (char *)err_host + 8, 8);
   if (err_host[0] & kErrArena) return fail(DSM_ERR_OOM, "adjacency arena full (relocation failed)");
   if (match_rc) return match_rc;
   float ms_total = 0, ms_match = 0, ms_upd = 0;
-  cudaEventElapsedTime(&ms_total, ev0, ev_end);
-  cudaEventElapsedTime(&ms_match, ev_m0, ev_m1);
-  cudaEventElapsedTime(&ms_upd, ev0, ev_upd);
+  elapsed(ev0, ev_end, &ms_total);
+  elapsed(ev_m0, ev_m1, &ms_match);
+  elapsed(ev0, ev_upd, &ms_upd);
 
   // ---- assemble the result view: counts, offsets, canonical order
   R.n = n;
@@ -795,7 +827,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
   stats.last_filter_ms = 0;
   if (filter_timed) {
     float fm = 0;
-    cudaEventElapsedTime(&fm, ev_pool[5], ev_pool[6]);
+    elapsed(ev_pool[5], ev_pool[6], &fm);
     stats.last_filter_ms = fm;
     filter_timed = false;
   }
@@ -858,7 +890,7 @@ int Engine::autotune(MatchArgs &ma, unsigned long long seed_cap, size_t nseg, in
     CK(cudaStreamSynchronize(stream));
     if (hs->error) break;  // keep the current setting
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
+    elapsed(e0, e1, &ms);
     stats.tune_runs++;
     if (k >= 0 && ms < best) {
       best = ms;
@@ -951,8 +983,10 @@ int Engine::launch_filter(uint32_t id, int mode) {
 
 // Candidate filters of every live query on the batch's union graph (sound
 // for every state the batch passes through); the matcher and the seeds then
-// test each candidate against its query vertex's bitmap.
-int Engine::run_filters() {
+// test each candidate against its query vertex's bitmap.  prepare_filters
+// (host: buffers, plans, descriptors) runs before the batch's device work;
+// launch_filters only enqueues kernels and events.
+int Engine::prepare_filters() {
   bool changed = false;
   for (uint32_t id : live_ids) {
     QDev &q = qd_host[id];
@@ -968,13 +1002,75 @@ int Engine::run_filters() {
   }
   if (changed)
     if (int rc = upload_qd()) return rc;
+  if (changed) CK(cudaStreamSynchronize(stream));  // qd_host is pageable
+  return DSM_OK;
+}
+
+int Engine::launch_filters() {
   if (filter_mode == 0) return DSM_OK;
   cudaEvent_t f0 = ev_pool[5], f1 = ev_pool[6];
-  CK(cudaEventRecord(f0, stream));
+  if (int r = rec(f0)) return r;
   for (uint32_t id : live_ids)
     if (int rc = launch_filter(id, filter_mode)) return rc;
-  CK(cudaEventRecord(f1, stream));
+  if (int r = rec(f1)) return r;
   filter_timed = true;
+  return DSM_OK;
+}
+
+// Records an event on the engine stream; while a segment is being captured
+// the record becomes a node of the graph (a plain record would only mark a
+// capture dependency and never time anything).
+int Engine::rec(cudaEvent_t ev) {
+  CK(cudaEventRecordWithFlags(ev, stream, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
+  return DSM_OK;
+}
+
+void Engine::elapsed(cudaEvent_t a, cudaEvent_t b, float *ms) {
+  if (cudaEventElapsedTime(ms, a, b) != cudaSuccess) {
+    cudaGetLastError();  // not recorded (e.g. no matcher launch): no time
+    *ms = 0;
+  }
+}
+
+// Captures fn's stream work into a graph and launches it through the
+// executable graph of segment k: updated in place when the topology is the
+// same as last time (the usual case: the same kernels with new sizes), else
+// instantiated anew.
+int Engine::run_segment(int k, const std::function<int()> &fn) {
+  CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  capturing = true;
+  const int rc = fn();
+  capturing = false;
+  cudaGraph_t gr = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(stream, &gr);
+  if (rc || e != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    cudaGetLastError();
+    return rc ? rc : cuda_fail(e, "graph capture");
+  }
+  bool updated = false;
+  if (gexec[k]) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(gexec[k], gr, &info) == cudaSuccess) {
+      updated = true;
+    } else {
+      cudaGetLastError();
+      cudaGraphExecDestroy(gexec[k]);
+      gexec[k] = nullptr;
+    }
+  }
+  if (!updated) {
+    const cudaError_t ei = cudaGraphInstantiate(&gexec[k], gr, 0);
+    if (ei != cudaSuccess) {
+      cudaGraphDestroy(gr);
+      gexec[k] = nullptr;
+      return cuda_fail(ei, "graph instantiate");
+    }
+    stats.graph_instantiations++;
+  }
+  cudaGraphDestroy(gr);
+  CK(cudaGraphLaunch(gexec[k], stream));
+  stats.graph_launches++;
   return DSM_OK;
 }
 

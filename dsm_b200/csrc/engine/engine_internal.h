@@ -8,6 +8,7 @@
 #include <condition_variable>
 #include <cstdint>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -117,6 +118,8 @@ struct Engine {
   int sort_results = 1;
   uint32_t split_min = 0, donate_depth = 0;  // donation granularity (0 = kernel default)
   bool tune_next = false;                    // autotune on the next batch
+  int use_graph = 0;                         // replay the batch segments as CUDA graphs
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool filter_timed = false;  // the filter events of this batch were recorded
   uint64_t result_cap = 1 << 20;
   uint32_t job_ring = 1 << 19;  // job slots of the matcher's donation ring
@@ -172,7 +175,12 @@ struct Engine {
   int retire_locked(uint32_t qid);                              // mu held
   int sync_queries();
   int upload_qd();
-  int run_filters();
+  int prepare_filters();
+  int launch_filters();
+  int run_segment(int k, const std::function<int()> &fn);
+  int rec(cudaEvent_t ev);
+  void elapsed(cudaEvent_t a, cudaEvent_t b, float *ms);
+  bool capturing = false;
   int prepare_filter(uint32_t id);
   int launch_filter(uint32_t id, int mode);
   int query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);

@@ -79,6 +79,10 @@ const char *dsm_last_error(dsm_engine *e);
                                    keeps the fastest in DSM_OPT_WARPS_PER_SM /
                                    DSM_OPT_SPLIT_MIN / DSM_OPT_DONATE_DEPTH; its results
                                    are those of any setting.  Reads 1 until that batch ran. */
+#define DSM_OPT_GRAPH 14        /* 1: each batch's two device segments (uploads .. matcher, and
+                                   deletes .. downloads) are captured into CUDA graphs and
+                                   launched through one executable graph per segment, updated
+                                   in place while the topology repeats (default 0) */
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
 int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
 
@@ -256,6 +260,8 @@ typedef struct dsm_stats {
   uint64_t live_queries;
   uint64_t tune_runs;        /* matcher launches timed by the autotuner */
   double tune_best_ms;       /* the fastest of them (last tuning) */
+  uint64_t graph_launches;   /* segment graphs launched (DSM_OPT_GRAPH) */
+  uint64_t graph_instantiations; /* of which needed a new executable graph */
 } dsm_stats;
 int dsm_engine_stats(dsm_engine *e, dsm_stats *s);
 

@@ -161,6 +161,43 @@ def test_autotuned_batch_equals_oracle():
     e.close()
 
 
+def test_graph_replay_equals_eager():
+    """DSM_OPT_GRAPH: the batch segments run as CUDA graphs (captured, then
+    updated in place while their topology repeats); listed results and the
+    graph equal the eager engine's, batch by batch."""
+    w = d.Workload(1)
+    q = w.queries[0]
+    eager, (qa,) = _fresh(w.nv, w.labels, w.edges, [q])
+    graph, (qb,) = _fresh(w.nv, w.labels, w.edges, [q], OPT_GRAPH=1)
+    ups = w.updates
+    for i in range(0, len(ups), 128):
+        ra, rb = eager.run_batch(ups[i:i + 128]), graph.run_batch(ups[i:i + 128])
+        assert np.array_equal(ra.signs, rb.signs) and np.array_equal(ra.counts, rb.counts)
+        assert np.array_equal(ra.tuples, rb.tuples)
+    for x, y in zip(eager.export_graph(), graph.export_graph()):
+        assert np.array_equal(x, y)
+    s = graph.stats()
+    nb = (len(ups) + 127) // 128
+    assert s["graph_launches"] == 2 * nb
+    assert s["graph_instantiations"] < s["graph_launches"]  # most batches update in place
+    eager.close()
+    graph.close()
+
+
+def test_graph_replay_with_filter_multi_query():
+    """Graph replay with the cluster filter inside the captured segment, 16
+    config-3 queries, against the oracle."""
+    w = d.Workload(3, scale_log2=-6, num_batches=2)
+    bs = [b[:512] for b in w.batches()]
+    qs = w.queries[:16]
+    e, qids = _fresh(w.nv, w.labels, w.edges, qs, OPT_GRAPH=1, OPT_FILTER=2)
+    streams = [oracle_stream(w.nv, w.labels, w.edges, q) for q in qs]
+    total, checked = run_stream(e, qids, streams, bs, check_graph_every=1, limit=200_000)
+    assert checked >= 16 * 256
+    assert e.stats()["graph_launches"] == 4
+    e.close()
+
+
 def test_listing_limit_downgrades_to_counts():
     w = d.Workload(1, scale_log2=-2)
     b = np.concatenate(list(w.batches())[:400])
