@@ -236,7 +236,8 @@ def run_serve(args):
     through three forms, each from the same initial graph.
       plain:   one engine per query, one launch per query per batch, in turn;
       batched: one engine, all queries in one launch per batch;
-      served:  one engine with the serving loop (continuous batching).
+      served:  one engine with the serving loop (continuous batching) and
+               CUDA-graph replay of each device batch.
     Phase 1 (burst): every request at t=0 -> throughput.  Phase 2 (the next
     requests): Poisson arrivals at 70% of the batched form's burst request
     rate -> p50 / p99 latency from arrival to results readable on the host."""
@@ -259,9 +260,10 @@ def run_serve(args):
           f"request sizes median {int(np.median([len(r) for r in reqs]))} max {max(len(r) for r in reqs)}",
           file=sys.stderr, flush=True)
 
-    def engine(qlist):
+    def engine(qlist, graph=False):
         e = d.Engine(0)
         e.set_option(d.OPT_LIST, args.list)
+        e.set_option(d.OPT_GRAPH, int(graph))
         e.load_graph_edges(w.nv, w.labels, w.edges)
         return e, [e.register(q) for q in qlist]
 
@@ -326,7 +328,7 @@ def run_serve(args):
     arms["batched"]["poisson"] = run_sync([(e, None)], arrivals, poisson)
     e.close()
     print(f"[serve] batched done; Poisson rate {rate:.1f} requests/s", file=sys.stderr, flush=True)
-    e, _ = engine(qs)
+    e, _ = engine(qs, graph=True)  # the served form replays its batch segments as CUDA graphs
     e.serve_start(args.serve_merge)
     arms["served"] = {"burst": run_served(e, np.zeros(K), burst), "poisson": run_served(e, arrivals, poisson)}
     e.serve_stop()
