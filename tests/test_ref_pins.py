@@ -1,0 +1,106 @@
+"""The oracle's restatements of decycle (decycle.cpp:6-135) and of the BFS
+matching order with backward neighbours (order.cpp:367-402, 647-676) against
+the reference's own code, compiled from its sources into oracle/_ref/libref.so
+by oracle/ref.mk (skipped where that library was not built).  No GPU.
+
+The reference reads a query's neighbour lists in file order
+(io.cu:181-189) and tests adjacency with a binary search over them
+(is_neighbor, order.h:9-27), so with a file whose edges are not listed in
+ascending (src < dst) order some backward neighbours go unseen.  The
+restatement tests true adjacency; on ascending files the two agree exactly,
+on other files the reference's masks are a subset of the restatement's."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "oracle", "_ref", "libref.so")
+pytestmark = pytest.mark.skipif(not os.path.exists(LIB), reason="oracle/_ref/libref.so not built")
+
+
+def _lib():
+    lib = C.CDLL(LIB)
+    u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+    u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+    lib.ref_decycle.argtypes = [C.c_uint32, C.c_uint32, u32p, u8p, u32p]
+    lib.ref_order.argtypes = [C.c_uint32, C.c_uint32, u32p, C.c_uint32, C.c_uint32, u32p, u32p]
+    return lib
+
+
+def _csr_file_order(nq, edges):
+    """Query CSR as readGraphToCPUDynamic fills it (io.cu:181-189)."""
+    deg = np.zeros(nq, np.int64)
+    for a, b in edges:
+        deg[a] += 1
+        deg[b] += 1
+    off = np.zeros(nq + 1, np.uint32)
+    off[1:] = np.cumsum(deg)
+    fill = off[:-1].astype(np.int64).copy()
+    nb = np.zeros(int(off[-1]), np.uint32)
+    for a, b in edges:
+        nb[fill[a]] = b
+        fill[a] += 1
+        nb[fill[b]] = a
+        fill[b] += 1
+    return off, nb
+
+
+def _random_query(rng, nq, extra):
+    extra = min(extra, nq * (nq - 1) // 2 - (nq - 1))
+    edges = set()
+    for v in range(1, nq):
+        edges.add((int(rng.integers(0, v)), v))
+    while len(edges) < nq - 1 + extra:
+        a, b = (int(x) for x in rng.integers(0, nq, 2))
+        if a != b and (a, b) not in edges and (b, a) not in edges:
+            edges.add((a, b))
+    edges = [e if rng.integers(0, 2) else (e[1], e[0]) for e in sorted(edges)]
+    perm = rng.permutation(nq)  # relabel so the tree root is not always 0
+    edges = [(int(perm[a]), int(perm[b])) for a, b in edges]
+    return [edges[i] for i in rng.permutation(len(edges))]
+
+
+def _queries(ascending):
+    rng = np.random.default_rng(2024)
+    qs = [(5, [(0, 1), (1, 2), (2, 0), (1, 3), (3, 4)])]  # the fixture query's shape
+    for _ in range(60):
+        nq = int(rng.integers(3, 13))
+        qs.append((nq, _random_query(rng, nq, int(rng.integers(0, nq)))))
+    if ascending:  # the order a file sorted by (src, dst) with src < dst lists them in
+        qs = [(nq, sorted(tuple(sorted(e)) for e in edges)) for nq, edges in qs]
+    return qs
+
+
+@pytest.mark.parametrize("ascending", [True, False])
+@pytest.mark.parametrize("k", range(61))
+def test_decycle_and_order_against_reference(k, ascending):
+    lib = _lib()
+    nq, edges = _queries(ascending)[k]
+    flat = np.array(edges, np.uint32).reshape(-1)
+    ne = len(edges)
+    qoff, qnbr = _csr_file_order(nq, edges)
+    # decycle: the same spanning tree and degrees
+    keep = np.zeros(ne, np.uint8)
+    deg = np.zeros(nq, np.uint32)
+    assert lib.ref_decycle(nq, ne, flat, keep, deg) == 0
+    ref_tree = {tuple(sorted(edges[e])) for e in range(ne) if keep[e]}
+    toff, tnbr, tdeg = orc.decycle(qoff, qnbr)
+    ours = {tuple(sorted((u, int(w)))) for u in range(nq) for w in tnbr[toff[u]:toff[u + 1]]}
+    assert ours == ref_tree
+    assert np.array_equal(tdeg, deg)
+    # matching order and backward neighbours for every ordered query edge
+    for a, b in edges:
+        for u, v in ((a, b), (b, a)):
+            ro = np.zeros(nq, np.uint32)
+            rb = np.zeros(nq, np.uint32)
+            assert lib.ref_order(nq, ne, flat, u, v, ro, rb) == 0
+            oo, ob = orc.order(qoff, qnbr, u, v)
+            assert np.array_equal(oo, ro), (u, v)
+            if ascending:
+                assert np.array_equal(ob, rb), (u, v)
+            else:
+                assert np.array_equal(ob & rb, rb), (u, v)  # the reference's masks miss some
