@@ -94,6 +94,7 @@ for _n in ("nv", "ne", "num_batches", "num_updates"):
 for _n in ("labels", "offsets", "nbrs", "edges", "batch_sizes"):
     _sig(f"dsm_text_{_n}", C.POINTER(C.c_uint32), P)
 _sig("dsm_text_updates", C.POINTER(C.c_uint32), P)
+_sig("dsm_text_write_binary", C.c_int, P, C.c_char_p)
 _sig("dsm_workload_generate", C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_uint32, C.POINTER(P))
 _sig("dsm_workload_free", None, P)
 _sig("dsm_workload_nv", C.c_uint32, P)
@@ -184,6 +185,22 @@ class TextGraph:
 
     def query(self):
         return Query(self.labels, self.offsets, self.nbrs)
+
+
+def to_binary(path, out_path, is_query):
+    """Converts a query or data file (text or binary) to the binary form,
+    which the engine and CDSM then map instead of parsing."""
+    h = P()
+    err = C.create_string_buffer(512)
+    rc = lib.dsm_text_read(path.encode(), int(is_query), C.byref(h), err, 512)
+    if rc:
+        raise DSMError(rc, err.value.decode())
+    try:
+        rc = lib.dsm_text_write_binary(h, out_path.encode())
+        if rc:
+            raise DSMError(rc, f"cannot write {out_path}")
+    finally:
+        lib.dsm_text_free(h)
 
 
 class Workload:

@@ -34,6 +34,7 @@ LIB_SOURCES = [
     "engine/noalloc.cu",
     "host/gen.cpp",
     "host/textio.cpp",
+    "host/binio.cpp",
     "host/query_plan.cpp",
 ]
 CLI_SOURCES = ["cli/cdsm.cpp"]

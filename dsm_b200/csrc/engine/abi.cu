@@ -12,7 +12,9 @@ struct dsm_engine {
   Engine e;
 };
 struct dsm_text {
-  dsm::TextGraph g;
+  dsm::TextGraph g;       // parsed text
+  dsm::MappedGraph m;     // or a mapped binary file
+  dsm::GraphArrays a;     // views of whichever holds the arrays
 };
 struct dsm_workload {
   dsm::Workload w;
@@ -310,7 +312,26 @@ int dsm_text_read(const char *path, int is_query, dsm_text **out, char *err, siz
   if (!path || !out) return DSM_ERR_ARG;
   auto *t = new dsm_text();
   std::string msg;
-  if (dsm::read_text_graph(path, is_query != 0, t->g, msg)) {
+  int bad;
+  if (dsm::is_binary_graph(path)) {
+    bad = dsm::map_binary_graph(path, is_query != 0, t->m, msg);
+    t->a = t->m.a;
+  } else {
+    bad = dsm::read_text_graph(path, is_query != 0, t->g, msg);
+    dsm::GraphArrays &a = t->a;
+    a.is_query = is_query != 0;
+    a.nv = t->g.nv;
+    a.ne = t->g.ne;
+    a.labels = t->g.labels.data();
+    a.offsets = t->g.offsets.data();
+    a.nbrs = t->g.nbrs.data();
+    a.edges = t->g.edges.data();
+    a.num_batches = (uint32_t)t->g.batch_sizes.size();
+    a.batch_sizes = t->g.batch_sizes.data();
+    a.num_updates = (uint32_t)(t->g.updates.size() / 4);
+    a.updates = t->g.updates.data();
+  }
+  if (bad) {
     if (err && err_len) {
       std::strncpy(err, msg.c_str(), err_len - 1);
       err[err_len - 1] = 0;
@@ -321,19 +342,24 @@ int dsm_text_read(const char *path, int is_query, dsm_text **out, char *err, siz
   *out = t;
   return DSM_OK;
 }
-void dsm_text_free(dsm_text *t) { delete t; }
-uint32_t dsm_text_nv(const dsm_text *t) { return t->g.nv; }
-uint32_t dsm_text_ne(const dsm_text *t) { return t->g.ne; }
-const uint32_t *dsm_text_labels(const dsm_text *t) { return t->g.labels.data(); }
-const uint32_t *dsm_text_offsets(const dsm_text *t) { return t->g.offsets.data(); }
-const uint32_t *dsm_text_nbrs(const dsm_text *t) { return t->g.nbrs.data(); }
-const uint32_t *dsm_text_edges(const dsm_text *t) { return t->g.edges.data(); }
-uint32_t dsm_text_num_batches(const dsm_text *t) { return (uint32_t)t->g.batch_sizes.size(); }
-const uint32_t *dsm_text_batch_sizes(const dsm_text *t) { return t->g.batch_sizes.data(); }
-uint32_t dsm_text_num_updates(const dsm_text *t) { return (uint32_t)(t->g.updates.size() / 4); }
-const dsm_update *dsm_text_updates(const dsm_text *t) {
-  return reinterpret_cast<const dsm_update *>(t->g.updates.data());
+
+int dsm_text_write_binary(const dsm_text *t, const char *path) {
+  if (!t || !path) return DSM_ERR_ARG;
+  std::string msg;
+  return dsm::write_binary_graph(path, t->a, msg) ? DSM_ERR_ARG : DSM_OK;
 }
+
+void dsm_text_free(dsm_text *t) { delete t; }
+uint32_t dsm_text_nv(const dsm_text *t) { return t->a.nv; }
+uint32_t dsm_text_ne(const dsm_text *t) { return t->a.ne; }
+const uint32_t *dsm_text_labels(const dsm_text *t) { return t->a.labels; }
+const uint32_t *dsm_text_offsets(const dsm_text *t) { return t->a.offsets; }
+const uint32_t *dsm_text_nbrs(const dsm_text *t) { return t->a.nbrs; }
+const uint32_t *dsm_text_edges(const dsm_text *t) { return t->a.edges; }
+uint32_t dsm_text_num_batches(const dsm_text *t) { return t->a.num_batches; }
+const uint32_t *dsm_text_batch_sizes(const dsm_text *t) { return t->a.batch_sizes; }
+uint32_t dsm_text_num_updates(const dsm_text *t) { return t->a.num_updates; }
+const dsm_update *dsm_text_updates(const dsm_text *t) { return reinterpret_cast<const dsm_update *>(t->a.updates); }
 
 // ---- workloads ---------------------------------------------------------------
 int dsm_workload_generate(int config, uint64_t seed, int scale_log2, uint32_t num_batches, dsm_workload **out) {

@@ -71,6 +71,26 @@ struct TextGraph {
   std::vector<uint32_t> updates;  // 4 words each
 };
 int read_text_graph(const std::string &path, bool is_query, TextGraph &g, std::string &err);
+
+// The arrays of a query or data file, however they are held (binio.cpp).
+struct GraphArrays {
+  bool is_query = false;
+  uint32_t nv = 0, ne = 0, num_batches = 0, num_updates = 0;
+  const uint32_t *labels = nullptr, *offsets = nullptr, *nbrs = nullptr, *edges = nullptr,
+                 *batch_sizes = nullptr, *updates = nullptr;
+};
+struct MappedGraph {
+  void *base = nullptr;
+  size_t len = 0;
+  GraphArrays a;
+  MappedGraph() = default;
+  MappedGraph(const MappedGraph &) = delete;
+  MappedGraph &operator=(const MappedGraph &) = delete;
+  ~MappedGraph();
+};
+bool is_binary_graph(const std::string &path);
+int write_binary_graph(const std::string &path, const GraphArrays &a, std::string &err);
+int map_binary_graph(const std::string &path, bool is_query, MappedGraph &m, std::string &err);
 int write_query_file(const std::string &path, const Query &q);
 int write_data_file(const std::string &path, const Workload &w);
 

@@ -270,6 +270,12 @@ typedef struct dsm_text dsm_text;
 /* readGraphToCPUDynamic (io.cu:122-252); is_query=1 stops after the graph. */
 int dsm_text_read(const char *path, int is_query, dsm_text **out, char *err, size_t err_len);
 void dsm_text_free(dsm_text *t);
+/* Binary form (no counterpart in the reference, whose `ifstream >>` text
+ * reader dominates load time at 2^28 edges): the arrays below behind a
+ * 64-byte header, each 64-byte aligned.  dsm_text_read recognises a binary
+ * file by its magic and maps it (mmap, no parsing, no copy); the arrays are
+ * those of the text file it was written from. */
+int dsm_text_write_binary(const dsm_text *t, const char *path);
 uint32_t dsm_text_nv(const dsm_text *t);
 uint32_t dsm_text_ne(const dsm_text *t);
 const uint32_t *dsm_text_labels(const dsm_text *t);

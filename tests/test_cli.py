@@ -62,3 +62,20 @@ def test_cli_generated_stream_matches_oracle(tmp_path):
         sign, cnt, tup = res[(i, 0)]
         assert cnt == counts[i] and sign == {1: "+", -1: "-", 0: "0"}[int(signs[i])]
         assert np.array_equal(np.array(tup, np.uint32).reshape(-1, q.nv), tuples[i])
+
+
+@pytest.mark.gpu
+def test_cli_binary_inputs_equal_text(tmp_path):
+    """CDSM on binary query and data files (mapped, not parsed) prints exactly
+    what it prints for the text files they were converted from."""
+    w = d.Workload(1, scale_log2=-2)
+    w.write(str(tmp_path / "q"), str(tmp_path / "g.in"))
+    d.to_binary(str(tmp_path / "q0.in"), str(tmp_path / "q0.bin"), True)
+    d.to_binary(str(tmp_path / "g.in"), str(tmp_path / "g.bin"), False)
+    outs = []
+    for q, g in (("q0.in", "g.in"), ("q0.bin", "g.bin")):
+        r = subprocess.run([d.CLI_PATH, "-q", str(tmp_path / q), "-d", str(tmp_path / g), "--gpu", "0"],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        outs.append(r.stdout)
+    assert outs[0] == outs[1] and outs[0].count("\nu ") > 100

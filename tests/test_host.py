@@ -54,6 +54,53 @@ def test_text_round_trip_generated(tmp_path):
     assert np.array_equal(q.offsets, w.queries[0].offsets) and np.array_equal(q.nbrs, w.queries[0].nbrs)
 
 
+def _same_graph(a, b):
+    for f in ("nv", "ne"):
+        assert getattr(a, f) == getattr(b, f)
+    for f in ("labels", "offsets", "nbrs", "edges", "batch_sizes", "updates"):
+        assert np.array_equal(getattr(a, f), getattr(b, f)), f
+
+
+def test_binary_round_trip(tmp_path):
+    """Text -> binary -> mapped: the same arrays as the text reader's, for a
+    data file with batches and for a query file; the fixture too."""
+    w = d.Workload(3, scale_log2=-8, num_batches=3)
+    w.write(str(tmp_path / "q"), str(tmp_path / "g.in"))
+    for src, is_q in ((tmp_path / "g.in", False), (tmp_path / "q0.in", True), (tmp_path / "q7.in", True),
+                      (os.path.join(ROOT, "tests", "golden", "example_g_01.in"), False),
+                      (os.path.join(ROOT, "tests", "golden", "example_q_01.in"), True)):
+        out = str(tmp_path / (os.path.basename(str(src)) + ".bin"))
+        d.to_binary(str(src), out, is_q)
+        with open(out, "rb") as f:
+            assert f.read(8) == b"DSMGRPH1"
+        _same_graph(d.TextGraph(str(src), is_q), d.TextGraph(out, is_q))
+        # converting the binary file again gives the same bytes
+        again = out + ".2"
+        d.to_binary(out, again, is_q)
+        assert open(out, "rb").read() == open(again, "rb").read()
+
+
+def test_binary_reader_errors(tmp_path):
+    w = d.Workload(1, scale_log2=-2)
+    w.write(str(tmp_path / "q"), str(tmp_path / "g.in"))
+    good = str(tmp_path / "g.bin")
+    d.to_binary(str(tmp_path / "g.in"), good, False)
+    data = open(good, "rb").read()
+    with pytest.raises(d.DSMError):  # a data graph where a query is expected
+        d.TextGraph(good, True)
+    cut = str(tmp_path / "cut.bin")
+    open(cut, "wb").write(data[:len(data) // 2])
+    with pytest.raises(d.DSMError):
+        d.TextGraph(cut, False)
+    bad = bytearray(data)
+    nv = int.from_bytes(bad[16:20], "little")
+    off0 = 64 + ((4 * nv + 63) // 64) * 64  # offsets section
+    bad[off0 + 4 * 1:off0 + 4 * 2] = (2 ** 31).to_bytes(4, "little")  # offsets[1] out of order
+    open(str(tmp_path / "bad.bin"), "wb").write(bytes(bad))
+    with pytest.raises(d.DSMError):
+        d.TextGraph(str(tmp_path / "bad.bin"), False)
+
+
 def test_text_reader_errors(tmp_path):
     p = tmp_path / "bad.in"
     p.write_text("t 2 1\nv 0 0 1\nv 1 0 2\ne 0 1\n")
