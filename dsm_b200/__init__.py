@@ -83,6 +83,8 @@ _sig("dsm_batch_release", C.c_int, P, C.c_uint64)
 _sig("dsm_engine_stats", C.c_int, P, C.POINTER(Stats))
 _sig("dsm_batch_timing_get", C.c_int, P, C.c_uint64, C.POINTER(BatchTiming))
 _sig("dsm_serve_start", C.c_int, P, C.c_uint32)
+_sig("dsm_engine_snapshot", C.c_int, P, C.c_char_p)
+_sig("dsm_engine_resume", C.c_int, P, C.c_char_p)
 _sig("dsm_serve_stop", C.c_int, P)
 _sig("dsm_query_register_async", C.c_int, P, u32p, u32p, u32p, C.c_uint32, C.POINTER(C.c_uint64))
 _sig("dsm_query_retire_async", C.c_int, P, C.c_uint32, C.POINTER(C.c_uint64))
@@ -383,6 +385,12 @@ class Engine:
         t = BatchTiming()
         self._ck(lib.dsm_batch_timing_get(self._h, bid, C.byref(t)))
         return {f: getattr(t, f) for f, _ in BatchTiming._fields_}
+
+    def snapshot(self, path):
+        self._ck(lib.dsm_engine_snapshot(self._h, path.encode()))
+
+    def resume(self, path):
+        self._ck(lib.dsm_engine_resume(self._h, path.encode()))
 
     # serving loop
     def serve_start(self, max_merge_updates=0):

@@ -30,6 +30,7 @@ LIB_SOURCES = [
     "engine/filter.cu",
     "engine/engine.cu",
     "engine/serve.cu",
+    "engine/snapshot.cu",
     "engine/abi.cu",
     "engine/noalloc.cu",
     "host/gen.cpp",

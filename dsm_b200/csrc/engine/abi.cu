@@ -292,6 +292,18 @@ int dsm_batch_release(dsm_engine *e, uint64_t batch_id) {
   return e->e.release(batch_id);
 }
 
+int dsm_engine_snapshot(dsm_engine *e, const char *path) {
+  ENGINE_OR_ARG(e);
+  if (!path) return DSM_ERR_ARG;
+  return e->e.snapshot(path);
+}
+
+int dsm_engine_resume(dsm_engine *e, const char *path) {
+  ENGINE_OR_ARG(e);
+  if (!path) return DSM_ERR_ARG;
+  return e->e.resume(path);
+}
+
 int dsm_engine_stats(dsm_engine *e, dsm_stats *s) {
   ENGINE_OR_ARG(e);
   if (!s) return DSM_ERR_ARG;

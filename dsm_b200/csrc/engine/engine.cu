@@ -259,6 +259,10 @@ DevGraph Engine::dev_graph() {
 
 int Engine::export_graph(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries) {
   std::lock_guard<std::mutex> lk(mu);
+  return export_graph_locked(offsets, nbrs, num_entries);
+}
+
+int Engine::export_graph_locked(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries) {
   if (!graph_loaded) return fail(DSM_ERR_STATE, "no graph loaded");
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
@@ -314,7 +318,7 @@ size_t Engine::query_bytes_allocated() const {
 // Admission against the budget: engine bytes not owned by queries + the
 // footprints of the admitted queries + this one.  *fits_later: it would fit
 // once every other query retired.
-int Engine::admit(QueryPlan &plan, uint32_t *qid, bool *fits_later) {
+int Engine::admit(QueryPlan &plan, uint32_t *qid, bool *fits_later, int64_t want_id) {
   const size_t foot = query_footprint(plan);
   const size_t base = bytes_in_use - std::min(bytes_in_use, query_bytes_allocated());
   size_t charged = 0;
@@ -324,13 +328,18 @@ int Engine::admit(QueryPlan &plan, uint32_t *qid, bool *fits_later) {
   if (base + charged + foot > budget)
     return fail(DSM_ERR_OOM, "query admission: footprint " + std::to_string(foot) + " bytes exceeds the budget");
   uint32_t id = (uint32_t)slots.size();
-  for (uint32_t i = 0; i < slots.size(); ++i)
-    if (!slots[i].live) {
-      id = i;
-      break;
-    }
+  if (want_id >= 0) {  // a resumed query keeps its id
+    id = (uint32_t)want_id;
+    if (id < slots.size() && slots[id].live) return fail(DSM_ERR_STATE, "query id already in use");
+  } else {
+    for (uint32_t i = 0; i < slots.size(); ++i)
+      if (!slots[i].live) {
+        id = i;
+        break;
+      }
+  }
   if (id >= (1u << 23)) return fail(DSM_ERR_LIMIT, "too many queries");
-  if (id == slots.size()) slots.emplace_back();
+  if (id >= slots.size()) slots.resize(id + 1);
   Slot &s = slots[id];
   s.live = true;
   s.plan = std::move(plan);

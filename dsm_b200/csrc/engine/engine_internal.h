@@ -166,12 +166,15 @@ struct Engine {
   uint32_t entry_of(uint32_t v) const { return pack_entry(label_host[v], v); }
   DevGraph dev_graph();
   int export_graph(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries);
+  int export_graph_locked(uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries);
+  int snapshot(const char *path);  // snapshot.cu
+  int resume(const char *path);
 
   int register_query(const uint32_t *qoff, const uint32_t *qnbr, const uint32_t *qlab, uint32_t nq, uint32_t *qid);
   int retire_query(uint32_t qid);
   size_t query_footprint(const QueryPlan &p) const;
   size_t query_bytes_allocated() const;
-  int admit(QueryPlan &plan, uint32_t *qid, bool *fits_later);  // mu held
+  int admit(QueryPlan &plan, uint32_t *qid, bool *fits_later, int64_t want_id = -1);  // mu held
   int retire_locked(uint32_t qid);                              // mu held
   int sync_queries();
   int upload_qd();

@@ -203,6 +203,18 @@ int dsm_query_retire_async(dsm_engine *e, uint32_t qid, uint64_t *ticket);
  * DSM_ERR_TIMEOUT while it still waits, else the request's error. */
 int dsm_query_admission(dsm_engine *e, uint64_t ticket, int64_t timeout_ms, uint32_t *qid);
 
+/* ---- snapshot / resume ---------------------------------------------- */
+/* No counterpart in the reference (its graph lives as long as one process).
+ * dsm_engine_snapshot writes the current data graph (sorted CSR and labels),
+ * every registered query with its id, and the batch counter to one file;
+ * taken between device batches, it covers exactly the batches that finished
+ * before it (queued ones are not in it).  dsm_engine_resume loads such a
+ * file into an engine with no registered queries and the serving loop
+ * stopped: afterwards the same update batches give the same results as on
+ * the engine that wrote it. */
+int dsm_engine_snapshot(dsm_engine *e, const char *path);
+int dsm_engine_resume(dsm_engine *e, const char *path);
+
 /* ---- counting without allocating ------------------------------------- */
 /* No counterpart in the reference: an entry point for callers that must not
  * allocate device memory while they run -- code living inside a framework

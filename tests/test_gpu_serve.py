@@ -143,3 +143,35 @@ def test_serving_errors_and_restart():
     r = e.run_batch(w.updates[:8])  # plain form again
     assert r.num_updates == 8 and qid in r.qids.tolist()
     e.close()
+
+
+def test_snapshot_resume(tmp_path):
+    """An engine resumed from a snapshot (graph, queries with their ids, batch
+    counter) gives the same results for the rest of the stream as the engine
+    that wrote it."""
+    w = d.Workload(1)
+    ups = w.updates
+    half = len(ups) // 2
+    a = d.Engine(0)
+    a.load_graph_edges(w.nv, w.labels, w.edges)
+    tri = d.Query.from_edges([0, 1, 2], [(0, 1), (1, 2), (0, 2)])
+    ids = [a.register(w.queries[0]), a.register(tri), a.register(tri)]
+    a.retire(ids[1])  # a hole in the ids
+    for i in range(0, half, 256):
+        a.run_batch(ups[i:min(i + 256, half)])
+    path = str(tmp_path / "engine.snap")
+    a.snapshot(path)
+    b = d.Engine(0)
+    b.resume(path)
+    for x, y in zip(a.export_graph(), b.export_graph()):
+        assert np.array_equal(x, y)
+    for i in range(half, len(ups), 256):
+        ra, rb = a.run_batch(ups[i:i + 256]), b.run_batch(ups[i:i + 256])
+        assert ra.batch_id == rb.batch_id
+        assert ra.qids.tolist() == rb.qids.tolist() == [ids[0], ids[2]]
+        assert np.array_equal(ra.signs, rb.signs) and np.array_equal(ra.counts, rb.counts)
+        assert np.array_equal(ra.tuples, rb.tuples)
+    with pytest.raises(d.DSMError):
+        b.resume(path)  # queries are registered now
+    a.close()
+    b.close()
