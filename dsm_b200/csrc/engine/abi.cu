@@ -46,7 +46,11 @@ int dsm_engine_destroy(dsm_engine *e) {
   return DSM_OK;
 }
 
-const char *dsm_last_error(dsm_engine *e) { return e ? e->e.last_error.c_str() : "null engine"; }
+const char *dsm_last_error(dsm_engine *e) {
+  static thread_local std::string text;  // valid until this thread's next call
+  text = e ? e->e.error_text() : "null engine";
+  return text.c_str();
+}
 
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
   ENGINE_OR_ARG(e);

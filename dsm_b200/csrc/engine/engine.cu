@@ -15,6 +15,8 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <thread>
+#include <atomic>
 
 #include "../../../include/dsm.h"
 #include "../host/dsm_host.h"
@@ -42,12 +44,12 @@ const char *status_string(int s) {
 }
 
 int Engine::fail(int code, const std::string &msg) {
-  last_error = msg;
+  set_error(msg);
   return code;
 }
 
 int Engine::cuda_fail(cudaError_t e, const char *where) {
-  last_error = std::string(where) + ": " + cudaGetErrorString(e);
+  set_error(std::string(where) + ": " + cudaGetErrorString(e));
   return DSM_ERR_CUDA;
 }
 
@@ -459,6 +461,40 @@ int Engine::upload_qd() {
 // ---------------------------------------------------------------------------
 // Batches
 // ---------------------------------------------------------------------------
+
+// Canonical order of the listed tuples: each (query, update) segment sorted
+// lexicographically, segments shared among host threads (largest first) when
+// the batch listed enough tuples to pay for the threads.
+void Engine::sort_segments(BatchResult &R, uint32_t nq_live, uint32_t n, size_t total) {
+  std::vector<uint32_t> segs;
+  for (size_t s = 0; s < (size_t)nq_live * n; ++s)
+    if (R.counts[s] >= 2) segs.push_back((uint32_t)s);
+  std::sort(segs.begin(), segs.end(), [&](uint32_t a, uint32_t b) { return R.counts[a] > R.counts[b]; });
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    std::vector<uint32_t> idx, tmp;
+    for (size_t k; (k = next.fetch_add(1)) < segs.size();) {
+      const size_t s = segs[k], c = R.counts[s];
+      const uint32_t w = R.widths[s / n];
+      uint32_t *base = &R.tuples[R.offsets[s]];
+      idx.resize(c);
+      for (size_t i = 0; i < c; ++i) idx[i] = (uint32_t)i;
+      std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+        return std::lexicographical_compare(base + (size_t)x * w, base + (size_t)x * w + w, base + (size_t)y * w,
+                                            base + (size_t)y * w + w);
+      });
+      tmp.resize(c * w);
+      for (size_t i = 0; i < c; ++i) std::memcpy(&tmp[i * w], base + (size_t)idx[i] * w, w * 4);
+      std::memcpy(base, tmp.data(), tmp.size() * 4);
+    }
+  };
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = total < (1u << 16) ? 1u : std::min<unsigned>(std::min(hw, 32u), (unsigned)segs.size());
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; ++t) th.emplace_back(work);
+  work();
+  for (auto &t : th) t.join();
+}
 int Engine::check_updates(const dsm_update *ups, uint32_t n) {
   if (!graph_loaded) return fail(DSM_ERR_STATE, "no graph loaded");
   if (n >= (1u << 30)) return fail(DSM_ERR_LIMIT, "batch larger than 2^30 updates");
@@ -520,7 +556,7 @@ int Engine::wait_batch(uint64_t id) {
   srv.done_cv.wait(q, [&] { return srv.done.count(id) != 0; });
   auto f = srv.failed.find(id);
   if (f != srv.failed.end()) {
-    last_error = f->second.msg;
+    set_error(f->second.msg);
     return f->second.rc;
   }
   return DSM_OK;
@@ -724,7 +760,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
     // more than the limit downgrades this batch to counts only
     if (listed && (double)sc.out_count.v * (ma.W + 1) * 4.0 > (double)list_limit_bytes) {
       listed = 0;
-      last_error = "batch listing exceeds the listing limit; returned counts only";
+      set_error("batch listing exceeds the listing limit; returned counts only");
       break;
     }
     if (!listed || sc.out_count.v <= ma.cap) break;
@@ -804,23 +840,7 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
       std::memcpy(&R.tuples[cur[s]], ht + r * ma.W, w * 4);
       cur[s] += w;
     }
-    if (sort_results) {
-      for (size_t s = 0; s < (size_t)nq_live * n; ++s) {
-        size_t c = R.counts[s];
-        if (c < 2) continue;
-        uint32_t w = R.widths[s / n];
-        uint32_t *base = &R.tuples[R.offsets[s]];
-        std::vector<uint32_t> idx(c);
-        for (size_t i = 0; i < c; ++i) idx[i] = (uint32_t)i;
-        std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
-          return std::lexicographical_compare(base + (size_t)x * w, base + (size_t)x * w + w, base + (size_t)y * w,
-                                              base + (size_t)y * w + w);
-        });
-        std::vector<uint32_t> tmp((size_t)c * w);
-        for (size_t i = 0; i < c; ++i) std::memcpy(&tmp[i * w], base + (size_t)idx[i] * w, w * 4);
-        std::memcpy(base, tmp.data(), tmp.size() * 4);
-      }
-    }
+    if (sort_results) sort_segments(R, nq_live, n, cnt);
   }
   stats.batches++;
   stats.updates += n;

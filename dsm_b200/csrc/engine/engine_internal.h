@@ -105,7 +105,16 @@ struct Engine {
   int clock_khz = 1965000;
   int match_blocks_per_sm = 2;
   std::mutex mu;
+  std::mutex emu;          // guards last_error (written by the serving worker too)
   std::string last_error;
+  void set_error(const std::string &m) {
+    std::lock_guard<std::mutex> lk(emu);
+    last_error = m;
+  }
+  std::string error_text() {
+    std::lock_guard<std::mutex> lk(emu);
+    return last_error;
+  }
   std::vector<cudaEvent_t> ev_pool;
 
   // options
@@ -193,6 +202,7 @@ struct Engine {
   int submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id);
   int run_batch(const dsm_update *ups, uint32_t n, BatchResult &R);
   int wait_batch(uint64_t id);
+  void sort_segments(BatchResult &R, uint32_t nq_live, uint32_t n, size_t total);
   int view(uint64_t id, dsm_result_view *v);
   int release(uint64_t id);
   int timing(uint64_t id, dsm_batch_timing *t);

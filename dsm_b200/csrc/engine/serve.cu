@@ -89,7 +89,7 @@ int Engine::admission(uint64_t ticket, int64_t timeout_ms, uint32_t *qid) {
     return DSM_ERR_TIMEOUT;
   const Outcome &o = srv.tickets[ticket];
   if (o.rc) {
-    last_error = o.msg;
+    set_error(o.msg);
     return o.rc;
   }
   *qid = o.qid;
@@ -114,7 +114,7 @@ void Engine::admit_pending() {
       srv.pending.push_front(std::move(r));
       return;
     }
-    srv.tickets[r.id] = Outcome{rc, qid, rc ? last_error : std::string()};
+    srv.tickets[r.id] = Outcome{rc, qid, rc ? error_text() : std::string()};
     srv.done_cv.notify_all();
   }
 }
@@ -125,7 +125,7 @@ Outcome Engine::handle_control(Request &r) {
   if (r.kind == kReqRetire) {
     o.rc = retire_locked(r.qid);
     o.qid = r.qid;
-    if (o.rc) o.msg = last_error;
+    if (o.rc) o.msg = error_text();
     admit_pending();
     return o;
   }
@@ -145,7 +145,7 @@ Outcome Engine::handle_control(Request &r) {
     o.rc = -1;  // no outcome yet
     return o;
   }
-  if (o.rc) o.msg = last_error;
+  if (o.rc) o.msg = error_text();
   return o;
 }
 
@@ -199,7 +199,7 @@ void Engine::run_merged(std::vector<Request> &reqs) {
     t0 = std::chrono::steady_clock::now();
     cudaSetDevice(device);
     rc = run_batch(all.data(), N, R);
-    if (rc) msg = last_error;
+    if (rc) msg = error_text();
   }
   if (rc) {
     std::lock_guard<std::mutex> q(srv.qmu);

@@ -53,7 +53,8 @@ typedef struct dsm_update {
 int dsm_engine_create(int device, size_t mem_budget, dsm_engine **out);
 int dsm_engine_destroy(dsm_engine *e);
 const char *dsm_status_string(int status);
-/* Text of the last error on this engine ("" if none). */
+/* Text of the last error on this engine ("" if none); the pointer stays
+ * valid until the calling thread's next dsm_last_error. */
 const char *dsm_last_error(dsm_engine *e);
 
 /* Options (dsm_engine_set_option). */
