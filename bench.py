@@ -93,6 +93,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def combine_over_ranks(dev_ms, wall_ms, matches, device):
+    """Whole-job figures of a replicated run: the slowest rank's times and the
+    matches of all ranks (one all-reduce each; every rank calls it)."""
+    import torch
+    t = torch.tensor([dev_ms, wall_ms, float(matches)], dtype=torch.float64, device=device)
+    mx = t.clone()
+    torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+    sm = t.clone()
+    torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
+    return float(mx[0]), float(mx[1]), int(sm[2])
+
+
 def make_workload(steps, warmup, scale):
     import dsm_b200 as d
     nb = steps + warmup
@@ -181,12 +193,7 @@ def run_ours(args, rank, world):
     h2d = int(sum(r[6] for r in rows) / len(rows))
     d2h = int(sum(r[7] for r in rows) / len(rows))
     if world > 1:
-        t = torch.tensor([dev_ms, wall_ms, matches], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
-        sm = t.clone()
-        torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
-        dev_ms, wall_ms, matches = float(mx[0]), float(mx[1]), int(sm[2])
+        dev_ms, wall_ms, matches = combine_over_ranks(dev_ms, wall_ms, matches, "cuda")
     if rank != 0:
         return None
     peak, peak_kind = _peaks()

@@ -1,0 +1,61 @@
+"""The replicated (N > 1) bench path on CPU: two gloo ranks combine their
+figures the way bench.py does over NCCL, and the CPU reference arm under
+torchrun runs on rank 0 only.  No GPU."""
+import datetime
+import json
+import multiprocessing as mp
+import os
+import socket
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, ROOT)
+    import torch
+
+    import bench
+    torch.distributed.init_process_group("gloo", rank=rank, world_size=world,
+                                         timeout=datetime.timedelta(seconds=60))
+    try:
+        out.put((rank, bench.combine_over_ranks(10.0 + rank, 20.0 - rank, 100 * (rank + 1), "cpu")))
+    finally:
+        torch.distributed.destroy_process_group()
+
+
+def test_combine_over_ranks_gloo():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    # the slowest rank's device and wall times, the matches of both ranks
+    assert res[0] == res[1] == (11.0, 20.0, 300)
+
+
+def test_reference_arm_under_torchrun():
+    port = _free_port()
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                        "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+                        "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--scale", "-6",
+                        "--ref-step-s", "0.2"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] >= 0 and d["cpu_baseline"]["cores"] >= 1
