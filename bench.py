@@ -7,17 +7,23 @@ edges (10% withheld for re-insertion), 16 Zipf(1.2) labels; three 8-vertex
 random-walk queries (tree, one cycle, 14 edges); batches of 4096 updates,
 50% inserts from the withheld pool, 50% deletes of live edges.
 
-A step is one update batch matched against the three queries.  Forms:
+A step is one update batch matched against the three queries, exact counts
+per update (--list 1 lists and sorts the embeddings as well).  Forms:
   batched (default): one engine, all queries in one persistent launch;
   plain: one engine per query, one launch per query (the reference's
          one-query-per-process form).
+The first warm-up batch autotunes the matcher's launch setting (--autotune).
 
 Prints one JSON line.  `value` = delta-matches per second of device time
-(updates already resident; H2D of the next batch is not in the kernels'
-event window); `e2e` = the same through the C ABI with host buffers (host
-prep, H2D, matching, D2H, canonical result assembly) on the wall clock.
+(CUDA events around each batch's device work); `e2e` = the same through the
+C ABI with host buffers (host prep, H2D, matching, D2H, result assembly) on
+the wall clock; `cpu_baseline` = the oracle's all-cores matcher on a prefix
+of the first timed batch (counts).  --impl reference: the CPU arm (the same
+oracle port, all host threads, a bounded prefix of each timed batch).
+--mode serve: served vs batched vs plain on the config-4 request stream
+(throughput under a burst, p50 / p99 latency under Poisson arrivals).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode step|serve]
 """
 import argparse
 import json
