@@ -145,7 +145,7 @@ Outcome Engine::handle_control(Request &r) {
     o.rc = -1;  // no outcome yet
     return o;
   }
-  if (o.rc) o.msg = error_text();
+  if (o.rc) o.msg = behind ? "query admission: footprint exceeds the budget" : error_text();
   return o;
 }
 
