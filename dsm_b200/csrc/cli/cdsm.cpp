@@ -11,8 +11,13 @@
 // Options beyond the reference's three: --out FILE (default stdout),
 // --count (counts only, no embedding lines), --queries a,b,... (more query
 // files matched in the same launch; lines then start with the query's
-// position as `q<k>`), --quiet (no per-update output; timing only).
-// Timing goes to stderr, one line per batch and a summary.
+// position as `q<k>`), --quiet (no per-update output; timing only),
+// --serve (the serving loop: every batch is queued at once, batches queued
+// together run as one device batch; the output is the same), --graph (CUDA
+// graph replay of each batch), --autotune (the first batch tunes the
+// matcher's launch setting).  Timing goes to stderr, one line per batch
+// (submit to results; with --serve, as the serving loop measured it) and a
+// summary.
 #include <chrono>
 #include <cinttypes>
 #include <cstdio>
@@ -28,7 +33,7 @@ namespace {
 void usage() {
   std::fprintf(stderr,
                "usage: CDSM -q <query> -d <data> [--gpu N] [--out FILE] [--count] [--quiet]\n"
-               "            [--queries q2,q3,...]\n");
+               "            [--queries q2,q3,...] [--serve] [--graph] [--autotune]\n");
 }
 
 bool read_text(const std::string &path, int is_query, dsm_text **t) {
@@ -46,7 +51,7 @@ bool read_text(const std::string &path, int is_query, dsm_text **t) {
 int main(int argc, char **argv) {
   std::string qpath, dpath, out_path, extra;
   int gpu = 0;
-  bool count_only = false, quiet = false;
+  bool count_only = false, quiet = false, serve = false, graph = false, autotune = false;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     auto next = [&](std::string &dst) {
@@ -66,6 +71,9 @@ int main(int argc, char **argv) {
     else if (a == "--queries") next(extra);
     else if (a == "--count") count_only = true;
     else if (a == "--quiet") quiet = true;
+    else if (a == "--serve") serve = true;
+    else if (a == "--graph") graph = true;
+    else if (a == "--autotune") autotune = true;
     else if (a == "-h" || a == "--help") {
       usage();
       return 0;
@@ -106,6 +114,8 @@ int main(int argc, char **argv) {
     return 1;
   }
   if (count_only) dsm_engine_set_option(e, DSM_OPT_LIST, 0);
+  if (graph) dsm_engine_set_option(e, DSM_OPT_GRAPH, 1);
+  if (autotune) dsm_engine_set_option(e, DSM_OPT_AUTOTUNE, 1);
   auto fail = [&](int code) {
     std::fprintf(stderr, "CDSM: %s: %s\n", dsm_status_string(code), dsm_last_error(e));
     dsm_engine_destroy(e);
@@ -128,16 +138,28 @@ int main(int argc, char **argv) {
   }
   const dsm_update *ups = dsm_text_updates(g);
   const uint32_t *sizes = dsm_text_batch_sizes(g);
+  const uint32_t nb = dsm_text_num_batches(g);
   uint64_t pos = 0, total_matches = 0, total_updates = 0;
   double total_ms = 0;
-  for (uint32_t b = 0; b < dsm_text_num_batches(g); ++b) {
+  std::vector<uint64_t> queued(nb, 0);
+  const auto t_loop = std::chrono::steady_clock::now();
+  if (serve) {  // queue every batch; the serving loop merges what queues up
+    if ((rc = dsm_serve_start(e, 0))) return fail(rc);
+    for (uint32_t b = 0, p = 0; b < nb; p += sizes[b], ++b)
+      if ((rc = dsm_batch_submit(e, ups + p, sizes[b], &queued[b]))) return fail(rc);
+  }
+  for (uint32_t b = 0; b < nb; ++b) {
     uint32_t n = sizes[b];
     auto tb = std::chrono::steady_clock::now();
-    uint64_t id = 0;
-    if ((rc = dsm_batch_submit(e, ups + pos, n, &id))) return fail(rc);
+    uint64_t id = queued[b];
+    if (!serve && (rc = dsm_batch_submit(e, ups + pos, n, &id))) return fail(rc);
     dsm_result_view v;
     if ((rc = dsm_batch_results(e, id, &v))) return fail(rc);
     double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+    if (serve) {
+      dsm_batch_timing tm;
+      if (dsm_batch_timing_get(e, id, &tm) == DSM_OK) ms = tm.total_ms;
+    }
     uint64_t bm = 0;
     for (uint32_t ql = 0; ql < v.num_queries; ++ql)
       for (uint32_t i = 0; i < v.num_updates; ++i) bm += v.counts[(size_t)ql * v.num_updates + i];
@@ -165,11 +187,13 @@ int main(int argc, char **argv) {
     total_updates += n;
     pos += n;
   }
+  if (serve) dsm_serve_stop(e);
+  const double wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_loop).count();
   dsm_stats st;
   dsm_engine_stats(e, &st);
-  std::fprintf(stderr, "total: %" PRIu64 " updates, %" PRIu64 " matches, %.3f ms (%.3e matches/s), "
-               "device %.3f ms in the last batch\n",
-               total_updates, total_matches, total_ms, total_ms > 0 ? total_matches / (total_ms / 1e3) : 0.0,
+  std::fprintf(stderr, "total: %" PRIu64 " updates, %" PRIu64 " matches, %.3f ms wall (%.3e matches/s), "
+               "batch latencies summed %.3f ms, device %.3f ms in the last device batch\n",
+               total_updates, total_matches, wall_ms, wall_ms > 0 ? total_matches / (wall_ms / 1e3) : 0.0, total_ms,
                st.last_batch_ms);
   if (out != stdout) std::fclose(out);
   for (auto *q : queries) dsm_text_free(q);

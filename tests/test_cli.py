@@ -79,3 +79,17 @@ def test_cli_binary_inputs_equal_text(tmp_path):
         assert r.returncode == 0, r.stderr
         outs.append(r.stdout)
     assert outs[0] == outs[1] and outs[0].count("\nu ") > 100
+
+
+@pytest.mark.gpu
+def test_cli_serve_and_graph_output_equal_plain(tmp_path):
+    """--serve (every batch queued at once, merged by the serving loop) with
+    --graph prints what the plain form prints, for two queries."""
+    w = d.Workload(1, scale_log2=-2)
+    w.write(str(tmp_path / "q"), str(tmp_path / "g.in"))
+    base = [d.CLI_PATH, "-q", str(tmp_path / "q0.in"), "-d", str(tmp_path / "g.in"), "--gpu", "0",
+            "--queries", str(tmp_path / "q0.in")]
+    plain = subprocess.run(base, capture_output=True, text=True)
+    served = subprocess.run(base + ["--serve", "--graph"], capture_output=True, text=True)
+    assert plain.returncode == 0 and served.returncode == 0, served.stderr
+    assert plain.stdout == served.stdout and plain.stdout.count("\nq1 u ") > 100
