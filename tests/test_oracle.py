@@ -158,3 +158,37 @@ def test_multithreaded_matcher_equals_sequential(qi):
     assert all(np.array_equal(x, y) for x, y in zip(t1, t2))
     for a, b in zip(one.export(), graph.export()):
         assert np.array_equal(a, b)
+
+
+def _embeddings(labels, adj, ql, qe):
+    """All embeddings by brute force (tiny graphs only)."""
+    import itertools
+    nq, nv = len(ql), len(labels)
+    out = []
+    for f in itertools.permutations(range(nv), nq):
+        if all(labels[f[u]] == ql[u] for u in range(nq)) and all(f[b] in adj[f[a]] for a, b in qe):
+            out.append(f)
+    return out
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_cluster_filter_is_sound(seed):
+    """The restated cluster filter (filter.cu) never drops a data vertex that
+    some embedding maps a query vertex to, and the LDF+NLF masks do not
+    either: the bitmaps are supersets of the true candidate sets."""
+    rng = np.random.default_rng(100 + seed)
+    nv = 11
+    labels, edges = _random_graph(rng, nv, 30, 2)
+    adj = [set() for _ in range(nv)]
+    for a, b in edges:
+        adj[a].add(int(b))
+        adj[b].add(int(a))
+    ql, qe = QUERIES[seed % len(QUERIES)]
+    qoff, qnb = _csr(len(ql), qe)
+    off, nb = _csr(nv, edges)
+    emb = _embeddings(labels, adj, ql, qe)
+    bm, vc, _, _ = orc.cluster_filter(np.array(ql, np.uint32), qoff, qnb, nv, labels, off, nb)
+    for f in emb:
+        for u, v in enumerate(f):
+            assert (bm[u][v // 32] >> (v % 32)) & 1, f"embedding {f}: vertex {v} pruned for u{u}"
+            assert (vc[v] >> u) & 1
