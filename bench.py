@@ -243,6 +243,79 @@ def run_ours(args, rank, world):
     return line
 
 
+def summarize(lat_ms, matches, updates, span_s):
+    lat = np.sort(np.asarray(lat_ms))
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "matches_per_sec": matches / span_s, "updates_per_sec": updates / span_s, "span_s": span_s,
+            "matches": int(matches)}
+
+
+def run_churn(e, arrivals, batch_list, live, pool):
+    """Poisson batches; every 4th arrival also registers a pool query or
+    retires a live one (alternately, keeping at least 4 live), through
+    the serving loop's queue.  Admission waits are timed per ticket."""
+    import random
+    rnd = random.Random(4)
+    bids, tickets, lock = [], [], threading.Lock()
+    counts = {"registrations": 0, "retirements": 0}
+    base = time.perf_counter()
+
+    def submitter():
+        for k, (a, b) in enumerate(zip(arrivals, batch_list)):
+            now = time.perf_counter() - base
+            if now < a:
+                time.sleep(a - now)
+            if k % 4 == 3:
+                with lock:
+                    retire = (k // 4) % 2 == 1 and len(live) > 4
+                    victim = live.pop(rnd.randrange(len(live))) if retire else None
+                if retire:
+                    e.retire_async(victim)
+                    counts["retirements"] += 1
+                else:
+                    tickets.append((e.register_async(pool[(k // 4) % len(pool)]), time.perf_counter()))
+                    counts["registrations"] += 1
+            bids.append(e.submit(b))
+
+    waits = []
+
+    def admitter():  # admission outcome of each registration, in order
+        k = 0
+        while k < len(tickets) or th.is_alive():
+            if k >= len(tickets):
+                time.sleep(0.001)
+                continue
+            t, t_sub = tickets[k]
+            qid = e.admission(t, 60_000)
+            waits.append((time.perf_counter() - t_sub) * 1e3)
+            if qid is not None:
+                with lock:
+                    live.append(qid)
+            k += 1
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    ta = threading.Thread(target=admitter)
+    ta.start()
+    lat, matches, upd = [], 0, 0
+    for k in range(len(batch_list)):
+        while len(bids) <= k:
+            time.sleep(0.0002)
+        t = e.timing(bids[k])
+        r = e.results(bids[k])
+        lat.append(t["total_ms"])
+        matches += int(r.counts.sum())
+        upd += r.num_updates
+    th.join()
+    ta.join()
+    out = summarize(lat, matches, upd, time.perf_counter() - base)
+    out.update(counts)
+    out["admission_wait_ms"] = {"p50": float(np.median(waits)) if waits else None,
+                                "max": float(max(waits)) if waits else None}
+    out["live_queries_at_end"] = e.stats()["live_queries"]
+    return out
+
+
 def run_serve(args):
     """Serving comparison on the config-4 stream (R-MAT, 32 uniform labels,
     lognormal batch sizes with median 512, 60% inserts): the same requests
@@ -253,7 +326,9 @@ def run_serve(args):
                CUDA-graph replay of each device batch.
     Phase 1 (burst): every request at t=0 -> throughput.  Phase 2 (the next
     requests): Poisson arrivals at 70% of the batched form's burst request
-    rate -> p50 / p99 latency from arrival to results readable on the host."""
+    rate -> p50 / p99 latency from arrival to results readable on the host.
+    Phase 3 (served form only, the next requests): the same arrivals with
+    query registrations and retirements through the serving loop's queue."""
     import torch
 
     import dsm_b200 as d
@@ -261,10 +336,10 @@ def run_serve(args):
     K = args.serve_requests
     scale = args.scale if args.scale else -6
     t0 = time.time()
-    w = d.Workload(4, scale_log2=scale, num_batches=2 * K)
+    w = d.Workload(4, scale_log2=scale, num_batches=3 * K)
     gen_s = time.time() - t0
-    reqs = list(w.batches())[:2 * K]
-    burst, poisson = reqs[:K], reqs[K:]
+    reqs = list(w.batches())[:3 * K]
+    burst, poisson, churn = reqs[:K], reqs[K:2 * K], reqs[2 * K:]
     # 8-10-vertex random-walk queries through the R-MAT hubs carry up to
     # 10^11 embeddings per request at this scale; the serving comparison uses
     # the pool's queries of at most 7 vertices
@@ -279,12 +354,6 @@ def run_serve(args):
         e.set_option(d.OPT_GRAPH, int(graph))
         e.load_graph_edges(w.nv, w.labels, w.edges)
         return e, [e.register(q) for q in qlist]
-
-    def summarize(lat_ms, matches, updates, span_s):
-        lat = np.sort(np.asarray(lat_ms))
-        return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                "matches_per_sec": matches / span_s, "updates_per_sec": updates / span_s, "span_s": span_s,
-                "matches": int(matches)}
 
     def run_sync(engines, arrivals, batch_list):
         """One request at a time, in arrival order, through every engine."""
@@ -341,9 +410,13 @@ def run_serve(args):
     arms["batched"]["poisson"] = run_sync([(e, None)], arrivals, poisson)
     e.close()
     print(f"[serve] batched done; Poisson rate {rate:.1f} requests/s", file=sys.stderr, flush=True)
-    e, _ = engine(qs, graph=True)  # the served form replays its batch segments as CUDA graphs
+    e, ids = engine(qs, graph=True)  # the served form replays its batch segments as CUDA graphs
     e.serve_start(args.serve_merge)
     arms["served"] = {"burst": run_served(e, np.zeros(K), burst), "poisson": run_served(e, arrivals, poisson)}
+    # served only: the same arrivals with query churn (other forms would need
+    # engines to come and go; the live set differs, so no cross-form check)
+    pool = [q for q in w.queries if q.nv <= 7][args.serve_queries:] or qs
+    arms["served"]["churn"] = run_churn(e, arrivals, churn, list(ids), pool)
     e.serve_stop()
     e.close()
     print("[serve] served done", file=sys.stderr, flush=True)
