@@ -96,6 +96,7 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
       return DSM_OK;
     case DSM_OPT_AUTOTUNE: E.tune_next = value != 0; return DSM_OK;
     case DSM_OPT_GRAPH: E.use_graph = value ? 1 : 0; return DSM_OK;
+    case DSM_OPT_STALL_TEST: E.stall_test = value ? 1 : 0; return DSM_OK;
     case DSM_OPT_MEM_BUDGET:
       if (value <= 0 || (uint64_t)value < E.bytes_in_use)
         return E.fail(DSM_ERR_ARG, "budget must cover the bytes in use");
@@ -125,6 +126,7 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_DONATE_DEPTH: *value = E.donate_depth; return DSM_OK;
     case DSM_OPT_AUTOTUNE: *value = E.tune_next ? 1 : 0; return DSM_OK;
     case DSM_OPT_GRAPH: *value = E.use_graph; return DSM_OK;
+    case DSM_OPT_STALL_TEST: *value = E.stall_test; return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");
 }

@@ -520,6 +520,7 @@ int Engine::submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id) {
       q.lock();
       r.id = next_batch_id++;
       *batch_id = r.id;
+      srv.inflight.insert(r.id);
       srv.queue.push_back(std::move(r));
       srv.work_cv.notify_one();
       return DSM_OK;
@@ -541,23 +542,22 @@ int Engine::submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id) {
     std::lock_guard<std::mutex> r(rmu);
     results[id] = std::move(res);
   }
-  {
-    std::lock_guard<std::mutex> q(srv.qmu);
-    srv.done.insert(id);
-  }
   *batch_id = id;
   return DSM_OK;
 }
 
-// Blocks until batch `id` is done; its status.
+// Blocks until batch `id` is done; its status.  A failure is reported once,
+// then forgotten (a later call finds no such batch).
 int Engine::wait_batch(uint64_t id) {
   std::unique_lock<std::mutex> q(srv.qmu);
   if (id == 0 || id >= next_batch_id) return fail(DSM_ERR_NOT_FOUND, "no such batch");
-  srv.done_cv.wait(q, [&] { return srv.done.count(id) != 0; });
+  srv.done_cv.wait(q, [&] { return srv.inflight.count(id) == 0; });
   auto f = srv.failed.find(id);
   if (f != srv.failed.end()) {
-    set_error(f->second.msg);
-    return f->second.rc;
+    const Outcome o = f->second;
+    srv.failed.erase(f);
+    set_error(o.msg);
+    return o.rc;
   }
   return DSM_OK;
 }
@@ -707,7 +707,8 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
     if (int r = rec(ev_upd)) return r;
     if (int r = launch_filters()) return r;  // per query, on the union graph
     if (nq_live) launch_seeds(sa, stream);
-    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream);
+    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream,
+                      stall_test);
     return DSM_OK;
   };
   // the matcher launch and the read-back of its scheduler state
@@ -777,7 +778,8 @@ int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
     reset.nseeds = sc.nseeds;
     CK(cudaMemcpyAsync(d_sched.ptr, &reset, sizeof(reset), cudaMemcpyHostToDevice, stream));
     CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
-    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream);
+    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream,
+                      stall_test);
     ++stats.kernel_launches;
     CK(cudaStreamSynchronize(stream));
   }
@@ -894,7 +896,8 @@ int Engine::autotune(MatchArgs &ma, unsigned long long seed_cap, size_t nseg, in
     hs->nseeds = nseeds;
     CK(cudaMemcpyAsync(d_sched.ptr, hs, sizeof(Sched), cudaMemcpyHostToDevice, stream));
     CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
-    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream);
+    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream,
+                      stall_test);
     ++stats.kernel_launches;
     CK(cudaStreamSynchronize(stream));  // hs is read by the copy
     return DSM_OK;

@@ -89,8 +89,14 @@ struct Server {
   std::condition_variable work_cv, done_cv;
   std::deque<Request> queue;
   std::deque<Request> pending;
+  // Bookkeeping stays bounded by what is in flight or unreported: a ticket
+  // sits in open_tickets until its outcome is posted to `tickets`, and leaves
+  // `tickets` once dsm_query_admission reported it; a queued batch sits in
+  // `inflight` until its results (or failure) are final, and a failure leaves
+  // `failed` once a wait reported it.
+  std::set<uint64_t> open_tickets;
   std::map<uint64_t, Outcome> tickets;
-  std::set<uint64_t> done;               // batches whose results (or failure) are final
+  std::set<uint64_t> inflight;
   std::map<uint64_t, Outcome> failed;
   uint32_t max_merge = 65536;
   uint64_t next_ticket = 1;
@@ -128,6 +134,7 @@ struct Engine {
   uint32_t split_min = 0, donate_depth = 0;  // donation granularity (0 = kernel default)
   bool tune_next = false;                    // autotune on the next batch
   int use_graph = 0;                         // replay the batch segments as CUDA graphs
+  int stall_test = 0;                        // arm matcher launches with a task nobody finishes
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool filter_timed = false;  // the filter events of this batch were recorded
   uint64_t result_cap = 1 << 20;
@@ -217,6 +224,7 @@ struct Engine {
   void worker_loop();
   Outcome handle_control(Request &r);
   void admit_pending();
+  void post_outcome(uint64_t ticket, const Outcome &o);  // qmu held
   void run_merged(std::vector<Request> &reqs);
 };
 

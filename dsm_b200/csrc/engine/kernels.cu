@@ -227,6 +227,10 @@ __global__ void k_seeds(SeedArgs A) {
   if (A.vtp[i] == kNoView) return;
   uint4 u = A.upd[i];
   uint32_t a = u.y, b = u.z;
+  // the engine validates updates on the host; callers that pass their own
+  // device buffers (the allocation-free entry point) may not have: an id out
+  // of range or a self loop seeds nothing
+  if (a >= A.g.nv || b >= A.g.nv || a == b) return;
   uint32_t la = A.g.lab[a] & kLabelMask, lb = A.g.lab[b] & kLabelMask;
   if (la >= 32 || lb >= 32) return;
   uint32_t pb = la * 32 + lb;

@@ -84,10 +84,10 @@ struct MatchArgs {
   uint32_t split_min;
   uint32_t donate_depth;
 };
-// Arms a matcher launch: outstanding = seeds, every ring slot free for its
-// first position.
+// Arms a matcher launch: outstanding = seeds (+ phantom, a task nothing
+// finishes: a test hook), every ring slot free for its first position.
 void launch_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long long *job_seq, uint32_t job_ring,
-                       cudaStream_t s);
+                       cudaStream_t s, uint32_t phantom = 0);
 void launch_match(const MatchArgs &a, int blocks, cudaStream_t s);
 int match_max_blocks_per_sm();
 

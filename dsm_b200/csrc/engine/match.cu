@@ -420,8 +420,10 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
   flush();
 }
 
+// phantom = 1 adds one outstanding task that nothing finishes (a test of the
+// bounded waits: the launch then ends only through their timeouts).
 __global__ void k_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long long *job_seq,
-                             uint32_t job_ring) {
+                             uint32_t job_ring, uint32_t phantom) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   for (uint32_t s = i; s < job_ring; s += gridDim.x * blockDim.x) job_seq[s] = s;
   if (i == 0) {
@@ -430,8 +432,8 @@ __global__ void k_sched_init(Sched *sc, unsigned long long seed_cap, unsigned lo
       sc->nseeds = n = seed_cap;
       atomicOr(&sc->error, kErrSeeds);
     }
-    sc->outstanding.v = n;
-    sc->done.v = (n == 0) ? 1ull : 0ull;
+    sc->outstanding.v = n + phantom;
+    sc->done.v = (n + phantom == 0) ? 1ull : 0ull;
   }
 }
 
@@ -482,8 +484,8 @@ __global__ void __launch_bounds__(256, DSM_MATCH_MIN_BLOCKS) k_match(MatchArgs P
 }  // namespace
 
 void launch_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long long *job_seq, uint32_t job_ring,
-                       cudaStream_t s) {
-  k_sched_init<<<(job_ring + 255) / 256, 256, 0, s>>>(sc, seed_cap, job_seq, job_ring);
+                       cudaStream_t s, uint32_t phantom) {
+  k_sched_init<<<(job_ring + 255) / 256, 256, 0, s>>>(sc, seed_cap, job_seq, job_ring, phantom);
 }
 
 void launch_match(const MatchArgs &a, int blocks, cudaStream_t s) {

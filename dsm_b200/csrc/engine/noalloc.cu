@@ -100,9 +100,18 @@ extern "C" int dsm_count_edge_embeddings_noalloc(int device, uint32_t nv, const 
     cudaSetDevice(prev);
     return code;
   };
+  cudaStream_t s = (cudaStream_t)stream;
+  // after the first asynchronous call, a failure waits for the work already
+  // queued on the stream: it may still write the shared scratch and the
+  // caller's counts, and a retry must not overlap it
+  auto cuda_failed = [&]() {
+    cudaGetLastError();
+    cudaStreamSynchronize(s);
+    cudaGetLastError();
+    return done(DSM_ERR_CUDA);
+  };
   unsigned char *base = nullptr;
   if ((rc = scratch_of(device, &base))) return done(rc);
-  cudaStream_t s = (cudaStream_t)stream;
 
   // query descriptor, orders and the (label, label) -> ordered edge table
   QDev qd;
@@ -134,10 +143,7 @@ extern "C" int dsm_count_edge_embeddings_noalloc(int device, uint32_t nv, const 
                                                  cudaMemcpyHostToDevice, s) == cudaSuccess) &&
             (n == 0 || cudaMemsetAsync(vtp, 0, 4ull * n, s) == cudaSuccess) &&
             (n == 0 || cudaMemsetAsync(d_counts, 0, 8ull * n, s) == cudaSuccess);
-  if (!ok) {
-    cudaGetLastError();
-    return done(DSM_ERR_CUDA);
-  }
+  if (!ok) return cuda_failed();
 
   // the caller's graph: adj = {run start in 16-byte units, degree} per vertex
   DevGraph g;
@@ -177,14 +183,12 @@ extern "C" int dsm_count_edge_embeddings_noalloc(int device, uint32_t nv, const 
   ma.timeout_cycles = 5000ll * (long long)(clk_khz > 0 ? clk_khz : 1965000);
   int per_sm = std::max(1, std::min(match_max_blocks_per_sm(), 4));
   launch_match(ma, std::max(sms, 1) * per_sm, s);
-  if (cudaGetLastError() != cudaSuccess) return done(DSM_ERR_CUDA);
+  if (cudaGetLastError() != cudaSuccess) return cuda_failed();
 
   unsigned int error = 0;
   if (cudaMemcpyAsync(&error, &sc->error, sizeof(error), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess) {
-    cudaGetLastError();
-    return done(DSM_ERR_CUDA);
-  }
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return cuda_failed();
   if (error & kErrTimeout) return done(DSM_ERR_TIMEOUT);
   if (error & kErrSeeds) return done(DSM_ERR_OVERFLOW);
   return done(DSM_OK);

@@ -44,7 +44,7 @@ int Engine::serve_stop() {
   }
   srv.worker.join();
   std::lock_guard<std::mutex> q(srv.qmu);
-  for (Request &r : srv.pending) srv.tickets[r.id] = Outcome{DSM_ERR_OOM, 0, "serving stopped before admission"};
+  for (Request &r : srv.pending) post_outcome(r.id, Outcome{DSM_ERR_OOM, 0, "serving stopped before admission"});
   srv.pending.clear();
   srv.running = false;
   srv.stopping = false;
@@ -62,6 +62,7 @@ int Engine::register_async(const uint32_t *qoff, const uint32_t *qnbr, const uin
   std::lock_guard<std::mutex> q(srv.qmu);
   if (!srv.running || srv.stopping) return fail(DSM_ERR_STATE, "the serving loop is not running");
   r.id = *ticket = srv.next_ticket++;
+  srv.open_tickets.insert(r.id);
   srv.queue.push_back(std::move(r));
   srv.work_cv.notify_one();
   return DSM_OK;
@@ -75,19 +76,30 @@ int Engine::retire_async(uint32_t qid, uint64_t *ticket) {
   std::lock_guard<std::mutex> q(srv.qmu);
   if (!srv.running || srv.stopping) return fail(DSM_ERR_STATE, "the serving loop is not running");
   r.id = *ticket = srv.next_ticket++;
+  srv.open_tickets.insert(r.id);
   srv.queue.push_back(std::move(r));
   srv.work_cv.notify_one();
   return DSM_OK;
 }
 
+void Engine::post_outcome(uint64_t ticket, const Outcome &o) {
+  srv.tickets[ticket] = o;
+  srv.open_tickets.erase(ticket);
+}
+
+// Each outcome is reported once: afterwards the ticket is forgotten and a
+// second call for it returns DSM_ERR_NOT_FOUND.
 int Engine::admission(uint64_t ticket, int64_t timeout_ms, uint32_t *qid) {
   std::unique_lock<std::mutex> q(srv.qmu);
   if (ticket == 0 || ticket >= srv.next_ticket) return fail(DSM_ERR_NOT_FOUND, "no such ticket");
-  auto ready = [&] { return srv.tickets.count(ticket) != 0; };
+  auto ready = [&] { return srv.tickets.count(ticket) != 0 || srv.open_tickets.count(ticket) == 0; };
   if (timeout_ms < 0) srv.done_cv.wait(q, ready);
   else if (!srv.done_cv.wait_for(q, std::chrono::milliseconds(timeout_ms), ready))
     return DSM_ERR_TIMEOUT;
-  const Outcome &o = srv.tickets[ticket];
+  auto it = srv.tickets.find(ticket);
+  if (it == srv.tickets.end()) return fail(DSM_ERR_NOT_FOUND, "ticket outcome already reported");
+  const Outcome o = it->second;
+  srv.tickets.erase(it);
   if (o.rc) {
     set_error(o.msg);
     return o.rc;
@@ -114,7 +126,7 @@ void Engine::admit_pending() {
       srv.pending.push_front(std::move(r));
       return;
     }
-    srv.tickets[r.id] = Outcome{rc, qid, rc ? error_text() : std::string()};
+    post_outcome(r.id, Outcome{rc, qid, rc ? error_text() : std::string()});
     srv.done_cv.notify_all();
   }
 }
@@ -161,7 +173,7 @@ void Engine::worker_loop() {
       q.unlock();
       Outcome o = handle_control(r);
       q.lock();
-      if (o.rc != -1) srv.tickets[r.id] = o;
+      if (o.rc != -1) post_outcome(r.id, o);
       srv.done_cv.notify_all();
       continue;
     }
@@ -205,7 +217,7 @@ void Engine::run_merged(std::vector<Request> &reqs) {
     std::lock_guard<std::mutex> q(srv.qmu);
     for (Request &r : reqs) {
       srv.failed[r.id] = Outcome{rc, 0, msg};
-      srv.done.insert(r.id);
+      srv.inflight.erase(r.id);
     }
     return;
   }
@@ -252,7 +264,7 @@ void Engine::run_merged(std::vector<Request> &reqs) {
     }
   }
   std::lock_guard<std::mutex> q(srv.qmu);
-  for (Request &r : reqs) srv.done.insert(r.id);
+  for (Request &r : reqs) srv.inflight.erase(r.id);
 }
 
 }  // namespace dsm

@@ -84,6 +84,12 @@ const char *dsm_last_error(dsm_engine *e);
                                    deletes .. downloads) are captured into CUDA graphs and
                                    launched through one executable graph per segment, updated
                                    in place while the topology repeats (default 0) */
+#define DSM_OPT_STALL_TEST 15   /* test hook (default 0): 1 arms every matcher launch with one
+                                   extra outstanding task that no warp ever finishes, so the
+                                   launch ends only when its idle warps' bounded waits run out
+                                   (DSM_OPT_TIMEOUT_MS without progress) and the batch returns
+                                   DSM_ERR_TIMEOUT after applying its updates to the graph.
+                                   Tests the failure path without faulting the device. */
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
 int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
 
@@ -143,7 +149,9 @@ int dsm_query_plan(const uint32_t *q_offsets, const uint32_t *q_nbrs, const uint
  * the reference's plain form); with it (dsm_serve_start) the call only
  * queues the batch and returns its id. */
 int dsm_batch_submit(dsm_engine *e, const dsm_update *ups, uint32_t n, uint64_t *batch_id);
-/* Blocks until the batch's results are on the host. */
+/* Blocks until the batch's results are on the host.  A batch that failed
+ * reports its error to the first wait (or results / timing call) only; the
+ * engine then forgets it. */
 int dsm_batch_wait(dsm_engine *e, uint64_t batch_id);
 
 typedef struct dsm_result_view {
@@ -201,7 +209,9 @@ int dsm_query_register_async(dsm_engine *e, const uint32_t *q_offsets, const uin
 int dsm_query_retire_async(dsm_engine *e, uint32_t qid, uint64_t *ticket);
 /* Waits up to timeout_ms (< 0: no limit) for a ticket's outcome: DSM_OK
  * (with *qid: the admitted or retired query) once it took effect,
- * DSM_ERR_TIMEOUT while it still waits, else the request's error. */
+ * DSM_ERR_TIMEOUT while it still waits, else the request's error.  Each
+ * outcome is reported once; the engine then forgets the ticket and a second
+ * call for it returns DSM_ERR_NOT_FOUND. */
 int dsm_query_admission(dsm_engine *e, uint64_t ticket, int64_t timeout_ms, uint32_t *qid);
 
 /* ---- snapshot / resume ---------------------------------------------- */
@@ -230,7 +240,8 @@ int dsm_engine_resume(dsm_engine *e, const char *path);
  * For each update i, d_counts[i] = the number of embeddings of the query that
  * map some query edge onto {src, dst} in the graph with that edge present
  * (the count an insert of the edge would report; the op and label fields are
- * not read).  src must differ from dst.
+ * not read).  src and dst must be vertex ids < nv and differ: an update
+ * naming a vertex >= nv, or a self loop, counts 0 and reads no graph memory.
  *   graph: d_adj holds 2 words per vertex, {start of the vertex's run in
  *          16-byte units, degree}; the run d_arena[4*start .. 4*start+degree)
  *          lists its neighbours sorted ascending, without duplicates;

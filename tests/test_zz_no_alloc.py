@@ -8,6 +8,7 @@ allocates nothing.  Its counts must equal what the engine's regular path
 reports for the same edges, on two calls in a row (the second call reuses the
 static scratch the first one left behind).  This file is collected last."""
 import ctypes as C
+import time
 
 import numpy as np
 import pytest
@@ -53,13 +54,17 @@ def _engine_counts(w, q, pick):
     return counts
 
 
-def test_noalloc_counts_match_engine_twice():
-    torch = pytest.importorskip("torch")
-    lib = d.lib
-    f = lib.dsm_count_edge_embeddings_noalloc
+def _entry():
+    f = d.lib.dsm_count_edge_embeddings_noalloc
     f.restype = C.c_int
     f.argtypes = [C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                   C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+    return f
+
+
+def test_noalloc_counts_match_engine_twice():
+    torch = pytest.importorskip("torch")
+    f = _entry()
 
     w = d.Workload(1)
     q = w.queries[0]
@@ -93,4 +98,55 @@ def test_noalloc_counts_match_engine_twice():
     out = torch.zeros(4097, dtype=torch.int64, device=dev)
     rc = f(0, w.nv, t_adj.data_ptr(), t_arena.data_ptr(), t_lab.data_ptr(), q.offsets.ctypes.data,
            q.nbrs.ctypes.data, q.labels.ctypes.data, q.nv, big.data_ptr(), 4097, out.data_ptr(), C.c_void_p(stream))
+    assert rc == 5  # DSM_ERR_LIMIT
+
+
+def test_noalloc_edge_cases():
+    """Empty call, a query whose labels meet no edge (no seeds: the matcher
+    finishes at once), ids out of range and self loops (count 0, no graph
+    read), and a query above the 8-vertex limit (refused)."""
+    torch = pytest.importorskip("torch")
+    f = _entry()
+    w = d.Workload(1)
+    q = w.queries[0]
+    adj, arena = _device_graph(w.nv, w.edges)
+    dev = torch.device("cuda", 0)
+    t_adj = torch.from_numpy(adj.view(np.int32)).to(dev)
+    t_arena = torch.from_numpy(arena.view(np.int32)).to(dev)
+    t_lab = torch.from_numpy(w.labels.view(np.int32)).to(dev)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+    def call(qq, ups):
+        ups = np.asarray(ups, np.uint32).reshape(-1, 4)
+        t_ups = torch.from_numpy(ups.view(np.int32).reshape(-1).copy()).to(dev) if len(ups) else \
+            torch.zeros(4, dtype=torch.int32, device=dev)
+        out = torch.full((max(len(ups), 1),), -1, dtype=torch.int64, device=dev)
+        torch.cuda.synchronize()
+        rc = f(0, w.nv, t_adj.data_ptr(), t_arena.data_ptr(), t_lab.data_ptr(), qq.offsets.ctypes.data,
+               qq.nbrs.ctypes.data, qq.labels.ctypes.data, qq.nv, t_ups.data_ptr(), len(ups), out.data_ptr(),
+               stream)
+        return rc, out.cpu().numpy().view(np.uint64)[:len(ups)]
+
+    rc, _ = call(q, [])
+    assert rc == 0
+    # labels 0..3 only in the graph: a query of label 7 has no seed
+    q7 = d.Query(np.full(q.nv, 7, np.uint32), q.offsets, q.nbrs)
+    pick = w.edges[:64]
+    ups = np.zeros((64, 4), np.uint32)
+    ups[:, 0] = 1
+    ups[:, 1:3] = pick
+    t0 = time.perf_counter()
+    rc, got = call(q7, ups)
+    assert rc == 0 and not got.any()
+    assert time.perf_counter() - t0 < 2.0  # no bounded wait ran out
+    # a live edge, then ids >= nv and a self loop: those count 0
+    a, b = (int(x) for x in w.edges[0])
+    bad = [[1, a, b, 0], [1, w.nv, b, 0], [1, a, w.nv + 5, 0], [1, 0xFFFFFFFF, 0xFFFFFFFF, 0], [1, a, a, 0]]
+    rc, got = call(q, bad)
+    assert rc == 0
+    assert got[1:].tolist() == [0, 0, 0, 0]
+    assert got[0] == _engine_counts(w, q, np.array([[a, b]], np.uint32))[0]
+    # nine query vertices: beyond the stated maximum of eight
+    q9 = d.Query.from_edges(np.zeros(9, np.uint32), [(i, i + 1) for i in range(8)])
+    rc, _ = call(q9, ups[:4])
     assert rc == 5  # DSM_ERR_LIMIT
