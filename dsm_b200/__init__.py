@@ -19,7 +19,8 @@ ERR = {1: "PARSE", 2: "OOM", 3: "OVERFLOW", 4: "TIMEOUT", 5: "LIMIT", 6: "ARG", 
        9: "NOT_FOUND"}
 
 OPT_LIST, OPT_FILTER, OPT_RESULT_CAP, OPT_WARPS_PER_SM, OPT_DONATE, OPT_TIMEOUT_MS, OPT_LABEL_QUIRK, OPT_SORT, \
-    OPT_LIST_LIMIT, OPT_MEM_BUDGET, OPT_SPLIT_MIN, OPT_DONATE_DEPTH, OPT_AUTOTUNE, OPT_GRAPH = range(1, 15)
+    OPT_LIST_LIMIT, OPT_MEM_BUDGET, OPT_SPLIT_MIN, OPT_DONATE_DEPTH, OPT_AUTOTUNE, OPT_GRAPH, OPT_STALL_TEST, \
+    OPT_PLAIN, OPT_QUERY_LIST_LIMIT = range(1, 18)
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is not built; run `python dsm_b200/build.py`")
@@ -37,7 +38,8 @@ class ResultView(C.Structure):
     _fields_ = [("batch_id", C.c_uint64), ("num_updates", C.c_uint32), ("num_queries", C.c_uint32),
                 ("qids", C.POINTER(C.c_uint32)), ("widths", C.POINTER(C.c_uint32)),
                 ("signs", C.POINTER(C.c_int8)), ("counts", C.POINTER(C.c_uint64)),
-                ("offsets", C.POINTER(C.c_uint64)), ("tuples", C.POINTER(C.c_uint32)), ("listed", C.c_int)]
+                ("offsets", C.POINTER(C.c_uint64)), ("tuples", C.POINTER(C.c_uint32)), ("listed", C.c_int),
+                ("query_listed", C.POINTER(C.c_uint8))]
 
 
 class Stats(C.Structure):
@@ -46,7 +48,8 @@ class Stats(C.Structure):
                [(n, C.c_double) for n in ("last_batch_ms", "last_match_ms", "last_filter_ms", "last_update_ms",
                                           "last_sort_ms")] + [(n, C.c_uint64) for n in (
                    "device_bytes_in_use", "kernel_launches", "query_bytes", "live_queries", "tune_runs")] + \
-               [("tune_best_ms", C.c_double), ("graph_launches", C.c_uint64), ("graph_instantiations", C.c_uint64)]
+               [("tune_best_ms", C.c_double)] + [(n, C.c_uint64) for n in (
+                   "graph_launches", "graph_instantiations", "graph_captures", "compactions")]
 
 
 class BatchTiming(C.Structure):
@@ -71,6 +74,7 @@ _sig("dsm_graph_load", C.c_int, P, u32p, u32p, u32p, C.c_uint32)
 _sig("dsm_graph_load_edges", C.c_int, P, C.c_uint32, u32p, C.c_uint64, u32p)
 _sig("dsm_graph_export", C.c_int, P, P, P, C.POINTER(C.c_uint64))
 _sig("dsm_graph_info", C.c_int, P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
+_sig("dsm_graph_apply", C.c_int, P, P, C.c_uint32)
 _sig("dsm_query_register", C.c_int, P, u32p, u32p, u32p, C.c_uint32, C.POINTER(C.c_uint32))
 _sig("dsm_query_retire", C.c_int, P, C.c_uint32)
 _sig("dsm_query_order", C.c_int, P, C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p)
@@ -277,6 +281,7 @@ class BatchResult:
         self.offsets = _arr(view.offsets, nq * n + 1, np.uint64)
         self.tuples = _arr(view.tuples, int(self.offsets[-1]) if len(self.offsets) else 0)
         self.listed = bool(view.listed)
+        self.query_listed = _arr(view.query_listed, nq, np.uint8).astype(bool)
         self.num_updates = n
 
     def query_index(self, qid):
@@ -324,6 +329,16 @@ class Engine:
 
     def load_graph_csr(self, offsets, nbrs, labels):
         self._ck(lib.dsm_graph_load(self._h, _u32(offsets), _u32(nbrs), _u32(labels), len(labels)))
+
+    def apply_graph(self, updates):
+        """Applies updates to the device graph without matching."""
+        u = self.pack_updates(updates)
+        self._ck(lib.dsm_graph_apply(self._h, u.ctypes.data, len(u)))
+
+    def graph_info(self):
+        nv, ne, aw = C.c_uint32(), C.c_uint64(), C.c_uint64()
+        self._ck(lib.dsm_graph_info(self._h, C.byref(nv), C.byref(ne), C.byref(aw)))
+        return {"nv": nv.value, "num_entries": ne.value, "arena_words": aw.value}
 
     def export_graph(self):
         n = C.c_uint64()

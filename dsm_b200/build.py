@@ -29,6 +29,7 @@ LIB_SOURCES = [
     "engine/match.cu",
     "engine/filter.cu",
     "engine/engine.cu",
+    "engine/batch.cu",
     "engine/serve.cu",
     "engine/snapshot.cu",
     "engine/abi.cu",

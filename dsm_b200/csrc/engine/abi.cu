@@ -97,6 +97,11 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
     case DSM_OPT_AUTOTUNE: E.tune_next = value != 0; return DSM_OK;
     case DSM_OPT_GRAPH: E.use_graph = value ? 1 : 0; return DSM_OK;
     case DSM_OPT_STALL_TEST: E.stall_test = value ? 1 : 0; return DSM_OK;
+    case DSM_OPT_PLAIN: E.plain = value ? 1 : 0; return DSM_OK;
+    case DSM_OPT_QUERY_LIST_LIMIT:
+      if (value < 0) return E.fail(DSM_ERR_ARG, "per-query listing limit must be >= 0");
+      E.query_list_limit = (unsigned long long)value;
+      return DSM_OK;
     case DSM_OPT_MEM_BUDGET:
       if (value <= 0 || (uint64_t)value < E.bytes_in_use)
         return E.fail(DSM_ERR_ARG, "budget must cover the bytes in use");
@@ -127,6 +132,8 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_AUTOTUNE: *value = E.tune_next ? 1 : 0; return DSM_OK;
     case DSM_OPT_GRAPH: *value = E.use_graph; return DSM_OK;
     case DSM_OPT_STALL_TEST: *value = E.stall_test; return DSM_OK;
+    case DSM_OPT_PLAIN: *value = E.plain; return DSM_OK;
+    case DSM_OPT_QUERY_LIST_LIMIT: *value = (int64_t)E.query_list_limit; return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");
 }
@@ -166,6 +173,12 @@ int dsm_graph_load_edges(dsm_engine *e, uint32_t nv, const uint32_t *labels, uin
 int dsm_graph_export(dsm_engine *e, uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries) {
   ENGINE_OR_ARG(e);
   return e->e.export_graph(offsets, nbrs, num_entries);
+}
+
+int dsm_graph_apply(dsm_engine *e, const dsm_update *ups, uint32_t n) {
+  ENGINE_OR_ARG(e);
+  if (!ups && n) return DSM_ERR_ARG;
+  return e->e.graph_apply(ups, n);
 }
 
 int dsm_graph_info(dsm_engine *e, uint32_t *nv, uint64_t *num_entries, uint64_t *arena_words) {
@@ -314,6 +327,7 @@ int dsm_engine_stats(dsm_engine *e, dsm_stats *s) {
   ENGINE_OR_ARG(e);
   if (!s) return DSM_ERR_ARG;
   std::lock_guard<std::mutex> lk(e->e.mu);
+  std::lock_guard<std::mutex> ls(e->e.smu);
   *s = e->e.stats;
   s->device_bytes_in_use = e->e.bytes_in_use;
   s->query_bytes = s->live_queries = 0;

@@ -57,7 +57,7 @@ __device__ __forceinline__ const uint32_t *adj_list(const DevGraph &g, uint2 a) 
 struct DevBatchEdges {
   const unsigned long long *bkey;
   const uint32_t *binfo;
-  uint32_t n;
+  uint32_t n;  // keys (set by the matcher from the batch header)
 };
 
 __device__ __forceinline__ unsigned long long canon_key(uint32_t a, uint32_t b) {
@@ -134,8 +134,9 @@ struct Sched {
   unsigned long long donations;
   unsigned long long steals;
   unsigned long long alg_bytes;
+  unsigned long long matches;  // embeddings counted (listed or not)
   unsigned int error;
-  unsigned int pad[7];
+  unsigned int pad[5];
 };
 
 constexpr unsigned kErrTimeout = 1u;

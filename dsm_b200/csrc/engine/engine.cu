@@ -20,6 +20,7 @@
 
 #include "../../../include/dsm.h"
 #include "../host/dsm_host.h"
+#include "../host/par.h"
 #include "../host/query_plan.h"
 #include "engine_internal.h"
 #include "filter.cuh"
@@ -111,8 +112,14 @@ Engine::~Engine() {
   for (auto &x : gexec)
     if (x) cudaGraphExecDestroy(x);
   for (DevBuf *b : all_dev_bufs()) dfree(*b);
-  for (HostBuf *b : {&h_stage, &h_sched, &h_segcnt, &h_vtp, &h_out_seg, &h_out_tup})
+  for (HostBuf *b : {&h_sched, &h_qlisted})
     if (b->ptr) cudaFreeHost(b->ptr);
+  for (HostOut &H : hout) {
+    for (HostBuf *b : {&H.stage, &H.hdr, &H.segcnt, &H.vtp, &H.out_seg, &H.out_tup, &H.misc})
+      if (b->ptr) cudaFreeHost(b->ptr);
+    if (H.ev0) cudaEventDestroy(H.ev0);
+    if (H.ev_end) cudaEventDestroy(H.ev_end);
+  }
   for (auto &ev : ev_pool)
     if (ev) cudaEventDestroy(ev);
   if (stream) cudaStreamDestroy(stream);
@@ -122,7 +129,7 @@ std::vector<DevBuf *> Engine::all_dev_bufs() {
   std::vector<DevBuf *> v = {&d_lab, &d_adj, &d_cap, &d_arena, &d_arena_top, &d_loff, &d_qd, &d_orders,
                              &d_pair_off, &d_pair_ent, &d_upd, &d_bkey, &d_bidx, &d_binfo, &d_gflag,
                              &d_vtp, &d_dkey, &d_dhead, &d_dsel, &d_seeds, &d_sched, &d_jobs,
-                             &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc};
+                             &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc, &d_hdr, &d_qlisted};
   for (auto &q : slots) v.push_back(&q.bitmap);
   for (auto &q : slots) v.push_back(&q.filter_scratch);
   for (auto &q : slots) v.push_back(&q.filter_plan);
@@ -154,6 +161,7 @@ int Engine::init(int dev, size_t mem_budget) {
   if (int rc = dalloc(d_sched, sizeof(Sched))) return rc;
   if (int rc = dalloc(d_arena_top, 256)) return rc;
   if (int rc = dalloc(d_misc, 256)) return rc;
+  if (int rc = dalloc(d_hdr, 256)) return rc;
   if (int rc = halloc(h_sched, sizeof(Sched) + 64)) return rc;
   return DSM_OK;
 }
@@ -173,7 +181,7 @@ int Engine::load_graph(uint32_t nv_, const uint32_t *labels, std::vector<uint64_
   }
   const uint32_t nlt_ = nv_ ? label_slot(max_label) + 1 : 1;
   // canonical, deduplicated undirected edges
-  std::sort(keys.begin(), keys.end());
+  parallel_sort(keys);
   keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
   std::vector<uint32_t> deg(nv_, 0);
   for (uint64_t k : keys) {
@@ -191,7 +199,7 @@ int Engine::load_graph(uint32_t nv_, const uint32_t *labels, std::vector<uint64_
   }
   if (off16 > 0xFFFFFFFFull) return fail(DSM_ERR_LIMIT, "graph too large for 32-bit run offsets");
   uint64_t used_words = off16 * 4;
-  uint64_t arena_words = used_words + used_words / 4 + (1u << 20);
+  uint64_t arena_words = used_words + used_words / 4 + std::min<uint64_t>(used_words, 1u << 20);
   arena_words = (arena_words + 3) & ~3ull;
   // fill runs on the host (pinned) and upload once
   HostBuf stage;
@@ -207,17 +215,19 @@ int Engine::load_graph(uint32_t nv_, const uint32_t *labels, std::vector<uint64_
   }
   const size_t stride = nlt_ + 1;
   std::vector<uint32_t> loff((size_t)nv_ * stride);
-  for (uint32_t v = 0; v < nv_; ++v) {
-    uint32_t *run = h_arena + (uint64_t)adj[v].x * 4;
-    std::sort(run, run + deg[v]);
-    for (uint32_t i = deg[v]; i < cap[v]; ++i) run[i] = 0xFFFFFFFFu;
-    adj[v].y = deg[v];
-    uint32_t *t = loff.data() + (size_t)v * stride;
-    for (uint32_t sl = 0, i = 0; sl <= nlt_; ++sl) {
-      while (i < deg[v] && (run[i] >> kIdBits) < sl) ++i;
-      t[sl] = sl == nlt_ ? deg[v] : i;
+  parallel_for(nv_, 1u << 14, [&](size_t lo, size_t hi) {
+    for (size_t v = lo; v < hi; ++v) {
+      uint32_t *run = h_arena + (uint64_t)adj[v].x * 4;
+      std::sort(run, run + deg[v]);
+      for (uint32_t i = deg[v]; i < cap[v]; ++i) run[i] = 0xFFFFFFFFu;
+      adj[v].y = deg[v];
+      uint32_t *t = loff.data() + v * stride;
+      for (uint32_t sl = 0, i = 0; sl <= nlt_; ++sl) {
+        while (i < deg[v] && (run[i] >> kIdBits) < sl) ++i;
+        t[sl] = sl == nlt_ ? deg[v] : i;
+      }
     }
-  }
+  });
   int rc;
   if ((rc = dalloc(d_lab, (size_t)nv_ * 4)) || (rc = dalloc(d_adj, (size_t)nv_ * 8)) ||
       (rc = dalloc(d_cap, (size_t)nv_ * 4)) || (rc = dalloc(d_loff, loff.size() * 4)) ||
@@ -449,6 +459,7 @@ int Engine::sync_queries() {
   CK(cudaStreamSynchronize(stream));
   queries_dirty = false;
   qd_dirty = true;
+  ++query_gen;
   return DSM_OK;
 }
 
@@ -465,16 +476,17 @@ int Engine::upload_qd() {
 // Canonical order of the listed tuples: each (query, update) segment sorted
 // lexicographically, segments shared among host threads (largest first) when
 // the batch listed enough tuples to pay for the threads.
-void Engine::sort_segments(BatchResult &R, uint32_t nq_live, uint32_t n, size_t total) {
+void Engine::sort_segments(BatchResult &R, const std::vector<uint64_t> &counts, uint32_t nq_live, uint32_t n,
+                           size_t total) {
   std::vector<uint32_t> segs;
   for (size_t s = 0; s < (size_t)nq_live * n; ++s)
-    if (R.counts[s] >= 2) segs.push_back((uint32_t)s);
-  std::sort(segs.begin(), segs.end(), [&](uint32_t a, uint32_t b) { return R.counts[a] > R.counts[b]; });
+    if (counts[s] >= 2) segs.push_back((uint32_t)s);
+  std::sort(segs.begin(), segs.end(), [&](uint32_t a, uint32_t b) { return counts[a] > counts[b]; });
   std::atomic<size_t> next{0};
   auto work = [&]() {
     std::vector<uint32_t> idx, tmp;
     for (size_t k; (k = next.fetch_add(1)) < segs.size();) {
-      const size_t s = segs[k], c = R.counts[s];
+      const size_t s = segs[k], c = counts[s];
       const uint32_t w = R.widths[s / n];
       uint32_t *base = &R.tuples[R.offsets[s]];
       idx.resize(c);
@@ -546,6 +558,18 @@ int Engine::submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id) {
   return DSM_OK;
 }
 
+int Engine::graph_apply(const dsm_update *ups, uint32_t n) {
+  {
+    std::lock_guard<std::mutex> q(srv.qmu);
+    if (srv.running) return fail(DSM_ERR_STATE, "graph apply while the serving loop runs");
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (int rc = check_updates(ups, n)) return rc;
+  CK(cudaSetDevice(device));
+  BatchResult R;
+  return run_batch(ups, n, R, false);
+}
+
 // Blocks until batch `id` is done; its status.  A failure is reported once,
 // then forgotten (a later call finds no such batch).
 int Engine::wait_batch(uint64_t id) {
@@ -575,370 +599,6 @@ int Engine::timing(uint64_t id, dsm_batch_timing *t) {
   t->merged_requests = R.merged_requests;
   t->merged_updates = R.merged_updates;
   return DSM_OK;
-}
-
-int Engine::run_batch(const dsm_update *ups, uint32_t n, BatchResult &R) {
-  if (int rc = sync_queries()) return rc;
-  auto t_host0 = std::chrono::steady_clock::now();
-  const uint32_t nq_live = (uint32_t)live_ids.size();
-  // ---- host prep: sorted undirected keys and sorted directed pairs
-  std::vector<std::pair<uint64_t, uint32_t>> und;
-  und.reserve(n);
-  for (uint32_t i = 0; i < n; ++i) {
-    uint32_t a = ups[i].src, b = ups[i].dst;
-    if (a == b) continue;
-    uint64_t k = a < b ? ((uint64_t)a << 32) | b : ((uint64_t)b << 32) | a;
-    und.push_back({k, i});
-  }
-  std::sort(und.begin(), und.end());
-  const uint32_t m = (uint32_t)und.size();
-  std::vector<uint64_t> dir;
-  dir.reserve(2 * (size_t)m);
-  for (auto &e : und) {  // x << 32 | entry of y, so each group is in run order
-    uint32_t a = (uint32_t)(e.first >> 32), b = (uint32_t)e.first;
-    dir.push_back(((uint64_t)a << 32) | entry_of(b));
-    dir.push_back(((uint64_t)b << 32) | entry_of(a));
-  }
-  std::sort(dir.begin(), dir.end());
-  std::vector<uint32_t> dhead;
-  for (size_t j = 0; j < dir.size(); ++j)
-    if (j == 0 || (dir[j] >> 32) != (dir[j - 1] >> 32)) dhead.push_back((uint32_t)j);
-  const uint32_t ngroups = (uint32_t)dhead.size();
-  dhead.push_back((uint32_t)dir.size());
-
-  // ---- staging (pinned) and device buffers
-  const size_t up_bytes = (size_t)n * 16, bk_bytes = (size_t)m * 8, bi_bytes = (size_t)m * 4,
-               dk_bytes = dir.size() * 8, dh_bytes = dhead.size() * 4;
-  const size_t stage_bytes = up_bytes + bk_bytes + bi_bytes + dk_bytes + dh_bytes + 64;
-  int rc;
-  if ((rc = halloc(h_stage, stage_bytes))) return rc;
-  const size_t nn = std::max<uint32_t>(n, 1), mm = std::max<uint32_t>(m, 1), dd = std::max<size_t>(dir.size(), 1);
-  const unsigned long long seed_cap = (unsigned long long)nn * std::max<uint32_t>(max_bucket, 1);
-  const size_t nseg = (size_t)std::max<uint32_t>(nq_live, 1) * nn;
-  if ((rc = dalloc(d_upd, nn * 16)) || (rc = dalloc(d_bkey, mm * 8)) || (rc = dalloc(d_bidx, mm * 4)) ||
-      (rc = dalloc(d_binfo, mm * 4)) || (rc = dalloc(d_gflag, mm)) || (rc = dalloc(d_vtp, nn * 4)) ||
-      (rc = dalloc(d_dkey, dd * 8)) || (rc = dalloc(d_dhead, (dd + 1) * 4)) || (rc = dalloc(d_dsel, dd * 4)) ||
-      (rc = dalloc(d_seeds, seed_cap * 16)) || (rc = dalloc(d_segcnt, nseg * 8)))
-    return rc;
-  if (!d_jobs.ptr) {
-    if ((rc = dalloc(d_jobs, (size_t)job_ring * sizeof(JobRec))) || (rc = dalloc(d_job_seq, (size_t)job_ring * 8)))
-      return rc;
-  }
-  if (list_mode) {
-    size_t cap = std::max<uint64_t>(result_cap, 1024);
-    if ((rc = dalloc(d_out_seg, cap * 4)) || (rc = dalloc(d_out_tup, cap * std::max<uint32_t>(max_width, 1) * 4)))
-      return rc;
-  }
-  char *st = (char *)h_stage.ptr;
-  size_t o_up = 0, o_bk = up_bytes, o_bi = o_bk + bk_bytes, o_dk = o_bi + bi_bytes, o_dh = o_dk + dk_bytes;
-  std::memcpy(st + o_up, ups, up_bytes);
-  for (uint32_t j = 0; j < m; ++j) {
-    ((uint64_t *)(st + o_bk))[j] = und[j].first;
-    ((uint32_t *)(st + o_bi))[j] = und[j].second;
-  }
-  std::memcpy(st + o_dk, dir.data(), dk_bytes);
-  std::memcpy(st + o_dh, dhead.data(), dh_bytes);
-  auto t_host1 = std::chrono::steady_clock::now();
-  R.host_prep_ms = std::chrono::duration<double, std::milli>(t_host1 - t_host0).count();
-
-  cudaEvent_t ev0 = ev_pool[0], ev_upd = ev_pool[1], ev_m0 = ev_pool[2], ev_m1 = ev_pool[3], ev_end = ev_pool[4];
-  // what allocates, synchronises or copies pageable memory runs before the
-  // device segments, so that each segment can be captured into a CUDA graph
-  if (qd_dirty)
-    if ((rc = upload_qd())) return rc;
-  if ((rc = prepare_filters())) return rc;
-  if ((rc = halloc(h_segcnt, nseg * 8)) || (rc = halloc(h_vtp, nn * 4))) return rc;
-  unsigned int *err_host = (unsigned int *)((char *)h_sched.ptr + sizeof(Sched));  // pinned, 16 bytes
-
-  DevGraph g = dev_graph();
-  unsigned int *d_err = (unsigned int *)d_misc.ptr;
-  unsigned long long *d_reloc = (unsigned long long *)((char *)d_misc.ptr + 8);
-  EdgeStateArgs es{g, (const uint4 *)d_upd.ptr, (const unsigned long long *)d_bkey.ptr,
-                   (const uint32_t *)d_bidx.ptr, m, n, (uint32_t *)d_binfo.ptr, (uint8_t *)d_gflag.ptr,
-                   (uint32_t *)d_vtp.ptr};
-  AdjUpdateArgs au{g, (const unsigned long long *)d_dkey.ptr, (const uint32_t *)d_dhead.ptr, ngroups,
-                   (const unsigned long long *)d_bkey.ptr, (const uint8_t *)d_gflag.ptr, m,
-                   (uint32_t *)d_dsel.ptr, d_err, d_reloc};
-  SeedArgs sa{g, (const uint4 *)d_upd.ptr, (const uint32_t *)d_vtp.ptr, n, (const uint32_t *)d_pair_off.ptr,
-              (const uint32_t *)d_pair_ent.ptr, (const QDev *)d_qd.ptr, (const OrderRec *)d_orders.ptr,
-              (uint4 *)d_seeds.ptr, seed_cap, (Sched *)d_sched.ptr};
-  MatchArgs ma;
-  ma.g = g;
-  ma.bt = DevBatchEdges{(const unsigned long long *)d_bkey.ptr, (const uint32_t *)d_binfo.ptr, m};
-  ma.vtp = (const uint32_t *)d_vtp.ptr;
-  ma.n = n;
-  ma.qd = (const QDev *)d_qd.ptr;
-  ma.orders = (const OrderRec *)d_orders.ptr;
-  ma.seeds = (const uint4 *)d_seeds.ptr;
-  ma.sc = (Sched *)d_sched.ptr;
-  ma.jobs = (JobRec *)d_jobs.ptr;
-  ma.job_seq = (unsigned long long *)d_job_seq.ptr;
-  ma.job_ring = job_ring;
-  ma.W = std::max<uint32_t>(max_width, 1);
-  ma.seg_count = (unsigned long long *)d_segcnt.ptr;
-  ma.list = list_mode;
-  ma.donate = donate;
-  ma.timeout_cycles = (long long)timeout_ms * (long long)clock_khz;
-  ma.split_min = split_min;
-  ma.donate_depth = donate_depth;
-  int blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
-  auto set_out = [&]() {
-    ma.out_seg = (uint32_t *)d_out_seg.ptr;
-    ma.out_tup = (uint32_t *)d_out_tup.ptr;
-    ma.cap = list_mode ? d_out_seg.bytes / 4 : 0;
-    if (list_mode) ma.cap = std::min<unsigned long long>(ma.cap, d_out_tup.bytes / 4 / ma.W);
-  };
-  // segment A: uploads, edge state, union insert, filters, seeds, arming
-  auto seg_a = [&]() -> int {
-    if (int r = rec(ev0)) return r;
-    if (n) CK(cudaMemcpyAsync(d_upd.ptr, st + o_up, up_bytes, cudaMemcpyHostToDevice, stream));
-    if (m) {
-      CK(cudaMemcpyAsync(d_bkey.ptr, st + o_bk, bk_bytes, cudaMemcpyHostToDevice, stream));
-      CK(cudaMemcpyAsync(d_bidx.ptr, st + o_bi, bi_bytes, cudaMemcpyHostToDevice, stream));
-      CK(cudaMemcpyAsync(d_dkey.ptr, st + o_dk, dk_bytes, cudaMemcpyHostToDevice, stream));
-      CK(cudaMemcpyAsync(d_dhead.ptr, st + o_dh, dh_bytes, cudaMemcpyHostToDevice, stream));
-    }
-    CK(cudaMemsetAsync(d_vtp.ptr, 0xFF, nn * 4, stream));
-    CK(cudaMemsetAsync(d_sched.ptr, 0, sizeof(Sched), stream));
-    CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
-    CK(cudaMemsetAsync(d_misc.ptr, 0, 256, stream));
-    launch_edge_state(es, stream);
-    launch_adj_insert(au, stream);
-    if (int r = rec(ev_upd)) return r;
-    if (int r = launch_filters()) return r;  // per query, on the union graph
-    if (nq_live) launch_seeds(sa, stream);
-    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream,
-                      stall_test);
-    return DSM_OK;
-  };
-  // the matcher launch and the read-back of its scheduler state
-  auto match_launch = [&]() -> int {
-    set_out();
-    if (int r = rec(ev_m0)) return r;
-    if (nq_live) launch_match(ma, blocks, stream);
-    if (int r = rec(ev_m1)) return r;
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h_sched.ptr, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
-    return DSM_OK;
-  };
-  stats.kernel_launches += (m > 0) + (ngroups > 0) + (nq_live > 0 && n > 0) + 1 + (nq_live > 0);
-  const bool tuning = tune_next && nq_live;
-  const bool graphed = use_graph && !tuning;  // a tuning batch runs eagerly
-  if (graphed) {
-    if ((rc = run_segment(0, [&]() -> int {
-          int r = seg_a();
-          return r ? r : match_launch();
-        })))
-      return rc;
-  } else {
-    if ((rc = seg_a())) return rc;
-    if (tuning) {
-      tune_next = false;
-      if ((rc = autotune(ma, seed_cap, nseg, blocks))) return rc;
-    }
-    if ((rc = match_launch())) return rc;
-  }
-  CK(cudaStreamSynchronize(stream));
-  Sched sc;
-  int listed = list_mode;  // may drop to counts only for this batch
-  int match_rc = DSM_OK;   // a matcher failure still lets the batch's graph updates finish
-  for (int attempt = 0;; ++attempt) {
-    if (attempt > 0) {  // a rerun after the result table grew (eager)
-      if ((rc = match_launch())) return rc;
-      ++stats.kernel_launches;
-      CK(cudaStreamSynchronize(stream));
-    }
-    std::memcpy(&sc, h_sched.ptr, sizeof(Sched));
-    if (sc.error & kErrTimeout) {
-      match_rc = fail(DSM_ERR_TIMEOUT, "matcher: a bounded wait gave up");
-      break;
-    }
-    if (sc.error & kErrSeeds) {
-      match_rc = fail(DSM_ERR_OVERFLOW, "seed table overflow");
-      break;
-    }
-    // the counts are complete (the matcher counts past the capacity); listing
-    // more than the limit downgrades this batch to counts only
-    if (listed && (double)sc.out_count.v * (ma.W + 1) * 4.0 > (double)list_limit_bytes) {
-      listed = 0;
-      set_error("batch listing exceeds the listing limit; returned counts only");
-      break;
-    }
-    if (!listed || sc.out_count.v <= ma.cap) break;
-    if (attempt >= 2) {
-      match_rc = fail(DSM_ERR_OVERFLOW, "result table kept overflowing");
-      break;
-    }
-    // grow to the exact count and run the matcher again on the same union graph
-    ++stats.result_regrows;
-    result_cap = sc.out_count.v + sc.out_count.v / 8 + 1024;
-    if ((rc = dalloc(d_out_seg, result_cap * 4)) || (rc = dalloc(d_out_tup, result_cap * ma.W * 4))) return rc;
-    Sched reset;
-    std::memset(&reset, 0, sizeof(reset));
-    reset.nseeds = sc.nseeds;
-    CK(cudaMemcpyAsync(d_sched.ptr, &reset, sizeof(reset), cudaMemcpyHostToDevice, stream));
-    CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
-    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream,
-                      stall_test);
-    ++stats.kernel_launches;
-    CK(cudaStreamSynchronize(stream));
-  }
-  unsigned long long reloc = 0;
-  // ---- segment B: deletions, marks, results
-  const size_t cnt = (listed && match_rc == DSM_OK) ? (size_t)sc.out_count.v : 0;
-  if (cnt)
-    if ((rc = halloc(h_out_seg, cnt * 4)) || (rc = halloc(h_out_tup, cnt * ma.W * 4))) return rc;
-  auto seg_b = [&]() -> int {
-    launch_adj_delete(au, stream);
-    launch_clear_touch(g, (const uint4 *)d_upd.ptr, n, stream);
-    if (int r = rec(ev_end)) return r;
-    if (cnt) {
-      CK(cudaMemcpyAsync(h_out_seg.ptr, d_out_seg.ptr, cnt * 4, cudaMemcpyDeviceToHost, stream));
-      CK(cudaMemcpyAsync(h_out_tup.ptr, d_out_tup.ptr, cnt * ma.W * 4, cudaMemcpyDeviceToHost, stream));
-    }
-    CK(cudaMemcpyAsync(h_segcnt.ptr, d_segcnt.ptr, nseg * 8, cudaMemcpyDeviceToHost, stream));
-    CK(cudaMemcpyAsync(h_vtp.ptr, d_vtp.ptr, nn * 4, cudaMemcpyDeviceToHost, stream));
-    CK(cudaMemcpyAsync(err_host, d_misc.ptr, 16, cudaMemcpyDeviceToHost, stream));
-    return DSM_OK;
-  };
-  stats.kernel_launches += (ngroups > 0) + (n > 0);
-  if ((rc = graphed ? run_segment(1, seg_b) : seg_b())) return rc;
-  CK(cudaStreamSynchronize(stream));
-  std::memcpy(&reloc, (char *)err_host + 8, 8);
-  if (err_host[0] & kErrArena) return fail(DSM_ERR_OOM, "adjacency arena full (relocation failed)");
-  if (match_rc) return match_rc;
-  float ms_total = 0, ms_match = 0, ms_upd = 0;
-  elapsed(ev0, ev_end, &ms_total);
-  elapsed(ev_m0, ev_m1, &ms_match);
-  elapsed(ev0, ev_upd, &ms_upd);
-
-  // ---- assemble the result view: counts, offsets, canonical order
-  R.n = n;
-  R.qids = live_ids;
-  R.widths.clear();
-  for (uint32_t id : live_ids) R.widths.push_back(slots[id].plan.nq);
-  R.signs.assign(n, 0);
-  const uint32_t *vtp = (const uint32_t *)h_vtp.ptr;
-  for (uint32_t i = 0; i < n; ++i)
-    if (vtp[i] != kNoView) R.signs[i] = ups[i].op ? 1 : -1;
-  R.counts.assign((size_t)nq_live * n, 0);
-  const unsigned long long *segc = (const unsigned long long *)h_segcnt.ptr;
-  for (size_t s = 0; s < (size_t)nq_live * n; ++s) R.counts[s] = segc[s];
-  R.offsets.assign((size_t)nq_live * n + 1, 0);
-  for (uint32_t ql = 0; ql < nq_live; ++ql)
-    for (uint32_t i = 0; i < n; ++i) {
-      size_t s = (size_t)ql * n + i;
-      R.offsets[s + 1] = R.offsets[s] + (listed ? R.counts[s] * R.widths[ql] : 0);
-    }
-  R.listed = listed;
-  R.tuples.clear();
-  if (listed) {
-    R.tuples.resize(R.offsets.back());
-    std::vector<uint64_t> cur(R.offsets.begin(), R.offsets.end() - 1);
-    const uint32_t *hs = (const uint32_t *)h_out_seg.ptr, *ht = (const uint32_t *)h_out_tup.ptr;
-    for (size_t r = 0; r < cnt; ++r) {
-      uint32_t s = hs[r];
-      uint32_t w = R.widths[s / n];
-      std::memcpy(&R.tuples[cur[s]], ht + r * ma.W, w * 4);
-      cur[s] += w;
-    }
-    if (sort_results) sort_segments(R, nq_live, n, cnt);
-  }
-  stats.batches++;
-  stats.updates += n;
-  stats.matches += sc.out_count.v;
-  stats.seeds += sc.nseeds;
-  stats.donations += sc.donations;
-  stats.steals += sc.steals;
-  stats.relocations += reloc;
-  stats.alg_bytes += sc.alg_bytes;
-  stats.last_batch_ms = ms_total;
-  stats.last_match_ms = ms_match;
-  stats.last_update_ms = ms_upd;
-  stats.last_filter_ms = 0;
-  if (filter_timed) {
-    float fm = 0;
-    elapsed(ev_pool[5], ev_pool[6], &fm);
-    stats.last_filter_ms = fm;
-    filter_timed = false;
-  }
-  R.device_ms = ms_total;
-  R.match_ms = ms_match;
-  R.alg_bytes = sc.alg_bytes;
-  R.matches = sc.out_count.v;
-  return DSM_OK;
-}
-
-// Autotuner: the matcher's result does not depend on its launch shape or on
-// how work is donated, so the batch's own matcher launch is repeated on the
-// same union graph (counts only) for each candidate -- resident blocks per SM
-// x range-split threshold x donation depth -- timed with events, and the
-// fastest becomes the engine's setting.  The first candidate runs twice and
-// its first run is not counted (it warms L2 for all).  Warps per task (1),
-// stack depth (the 16 lane-held levels) and the intersection tile (32
-// entries, one per lane) are fixed by the kernel's design.
-int Engine::autotune(MatchArgs &ma, unsigned long long seed_cap, size_t nseg, int &blocks) {
-  Sched *hs = (Sched *)h_sched.ptr;
-  CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
-  CK(cudaStreamSynchronize(stream));
-  if (hs->error) return DSM_OK;  // the real launch reports it
-  const unsigned long long nseeds = hs->nseeds;
-  struct Cand {
-    int bps;
-    uint32_t split, dd;
-  };
-  std::vector<Cand> cands;
-  for (int bps = std::max(1, match_blocks_per_sm - 2); bps <= match_blocks_per_sm; ++bps)
-    for (uint32_t split : {64u, 128u, 512u})
-      for (uint32_t dd : {1u, 2u}) cands.push_back({bps, split, dd});
-  auto rearm = [&]() -> int {
-    std::memset(hs, 0, sizeof(Sched));
-    hs->nseeds = nseeds;
-    CK(cudaMemcpyAsync(d_sched.ptr, hs, sizeof(Sched), cudaMemcpyHostToDevice, stream));
-    CK(cudaMemsetAsync(d_segcnt.ptr, 0, nseg * 8, stream));
-    launch_sched_init((Sched *)d_sched.ptr, seed_cap, (unsigned long long *)d_job_seq.ptr, job_ring, stream,
-                      stall_test);
-    ++stats.kernel_launches;
-    CK(cudaStreamSynchronize(stream));  // hs is read by the copy
-    return DSM_OK;
-  };
-  MatchArgs t = ma;
-  t.list = 0;
-  t.cap = 0;
-  float best = 1e30f;
-  Cand bc{blocks / std::max(num_sms, 1), ma.split_min, ma.donate_depth};
-  cudaEvent_t e0 = ev_pool[2], e1 = ev_pool[3];
-  for (int k = -1; k < (int)cands.size(); ++k) {
-    const Cand &c = cands[std::max(k, 0)];
-    if (int rc = rearm()) return rc;
-    t.split_min = c.split;
-    t.donate_depth = c.dd;
-    CK(cudaEventRecord(e0, stream));
-    launch_match(t, num_sms * c.bps, stream);
-    ++stats.kernel_launches;
-    CK(cudaEventRecord(e1, stream));
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
-    if (hs->error) break;  // keep the current setting
-    float ms = 0;
-    elapsed(e0, e1, &ms);
-    stats.tune_runs++;
-    if (k >= 0 && ms < best) {
-      best = ms;
-      bc = c;
-    }
-  }
-  if (best < 1e30f) {
-    warps_per_sm = bc.bps * 8;
-    split_min = bc.split;
-    donate_depth = bc.dd;
-    stats.tune_best_ms = best;
-  }
-  ma.split_min = split_min;
-  ma.donate_depth = donate_depth;
-  blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
-  return rearm();  // the batch's real launch starts from scratch
 }
 
 // Uploads the filter's descriptor and op list of query `id` and sizes its
@@ -993,6 +653,7 @@ int Engine::prepare_filter(uint32_t id) {
   CK(cudaStreamSynchronize(stream));  // `desc` and `ops` are stack / vector memory
   s.filter_nops = (uint32_t)ops.size();
   s.filter_dirty = false;
+  ++query_gen;
   return DSM_OK;
 }
 
@@ -1064,48 +725,6 @@ void Engine::elapsed(cudaEvent_t a, cudaEvent_t b, float *ms) {
   }
 }
 
-// Captures fn's stream work into a graph and launches it through the
-// executable graph of segment k: updated in place when the topology is the
-// same as last time (the usual case: the same kernels with new sizes), else
-// instantiated anew.
-int Engine::run_segment(int k, const std::function<int()> &fn) {
-  CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-  capturing = true;
-  const int rc = fn();
-  capturing = false;
-  cudaGraph_t gr = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(stream, &gr);
-  if (rc || e != cudaSuccess) {
-    if (gr) cudaGraphDestroy(gr);
-    cudaGetLastError();
-    return rc ? rc : cuda_fail(e, "graph capture");
-  }
-  bool updated = false;
-  if (gexec[k]) {
-    cudaGraphExecUpdateResultInfo info;
-    if (cudaGraphExecUpdate(gexec[k], gr, &info) == cudaSuccess) {
-      updated = true;
-    } else {
-      cudaGetLastError();
-      cudaGraphExecDestroy(gexec[k]);
-      gexec[k] = nullptr;
-    }
-  }
-  if (!updated) {
-    const cudaError_t ei = cudaGraphInstantiate(&gexec[k], gr, 0);
-    if (ei != cudaSuccess) {
-      cudaGraphDestroy(gr);
-      gexec[k] = nullptr;
-      return cuda_fail(ei, "graph instantiate");
-    }
-    stats.graph_instantiations++;
-  }
-  cudaGraphDestroy(gr);
-  CK(cudaGraphLaunch(gexec[k], stream));
-  stats.graph_launches++;
-  return DSM_OK;
-}
-
 int Engine::query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us) {
   std::lock_guard<std::mutex> lk(mu);
   if (!graph_loaded) return fail(DSM_ERR_STATE, "no graph loaded");
@@ -1139,6 +758,7 @@ int Engine::view(uint64_t id, dsm_result_view *v) {
   v->offsets = R.offsets.data();
   v->tuples = R.tuples.data();
   v->listed = R.listed;
+  v->query_listed = R.qlisted.data();
   return DSM_OK;
 }
 

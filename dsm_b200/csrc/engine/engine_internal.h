@@ -46,15 +46,49 @@ struct Slot {
   size_t foot = 0;           // device bytes charged to this query at admission
 };
 
+// Pinned host side of one device batch in flight (two sets, so the serving
+// loop can assemble batch k on the host while batch k + 1 runs).
+struct HostOut {
+  HostBuf stage;   // uploads: updates, sorted keys, indices, directed pairs, group heads
+  HostBuf hdr;     // BatchHdr
+  HostBuf segcnt, vtp, out_seg, out_tup, misc;
+  cudaEvent_t ev0 = nullptr, ev_end = nullptr;  // batch start, results downloaded
+};
+
+// One device batch from host preparation to result assembly.
+struct Staged {
+  const dsm_update *ups = nullptr;  // the caller's updates, valid until assemble
+  uint32_t n = 0, m = 0, ngroups = 0;
+  size_t ndir = 0;
+  size_t o_up = 0, o_bk = 0, o_bi = 0, o_dk = 0, o_dh = 0;  // offsets in the staging buffer
+  int slot = 0;
+  bool match = true;  // false: apply the updates to the graph only
+  double host_prep_ms = 0;
+  // fixed at launch
+  std::vector<uint32_t> qids, widths;
+  uint32_t nq_live = 0, W = 1;
+  size_t nseg = 0;
+  unsigned long long seed_cap = 0;
+  int plain = 0, sort = 1;
+  unsigned long long qlimit = 0;
+  // after the matcher
+  Sched sc{};
+  std::vector<unsigned long long> qlisted;
+  int listed = 0, match_rc = 0;
+  size_t cnt = 0;  // listed tuples downloaded
+  float ms_match = 0, ms_upd = 0, ms_filter = 0;
+};
+
 struct BatchResult {
   uint64_t id = 0;
   uint32_t n = 0;
   std::vector<uint32_t> qids, widths;
+  std::vector<uint8_t> qlisted;  // per query: its tuples are listed
   std::vector<int8_t> signs;
   std::vector<uint64_t> counts, offsets;
   std::vector<uint32_t> tuples;
   int listed = 1;
-  double device_ms = 0, match_ms = 0, host_prep_ms = 0;
+  double device_ms = 0, match_ms = 0, host_prep_ms = 0, sort_ms = 0;
   uint64_t alg_bytes = 0, matches = 0;
   // served timing: submit -> start of the device batch -> results readable
   double queue_ms = 0, service_ms = 0, total_ms = 0;
@@ -135,7 +169,12 @@ struct Engine {
   bool tune_next = false;                    // autotune on the next batch
   int use_graph = 0;                         // replay the batch segments as CUDA graphs
   int stall_test = 0;                        // arm matcher launches with a task nobody finishes
+  int plain = 0;                             // one matcher launch per query (the reference's form)
+  unsigned long long query_list_limit = 0;   // tuples one query may list per batch (0: no budget)
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  std::string gkey[2];                       // what each executable graph was captured with
+  uint64_t seg_kernels[2] = {0, 0};          // kernels each executable graph holds
+  uint64_t query_gen = 0;                    // bumped whenever the live queries or filters change
   bool filter_timed = false;  // the filter events of this batch were recorded
   uint64_t result_cap = 1 << 20;
   uint32_t job_ring = 1 << 19;  // job slots of the matcher's donation ring
@@ -159,8 +198,12 @@ struct Engine {
 
   // batch scratch
   DevBuf d_upd, d_bkey, d_bidx, d_binfo, d_gflag, d_vtp, d_dkey, d_dhead, d_dsel, d_seeds, d_sched, d_jobs,
-      d_job_seq, d_out_seg, d_out_tup, d_segcnt, d_misc;
-  HostBuf h_stage, h_sched, h_segcnt, h_vtp, h_out_seg, h_out_tup;
+      d_job_seq, d_out_seg, d_out_tup, d_segcnt, d_misc, d_hdr, d_qlisted;
+  HostBuf h_sched;    // Sched + the error words, read after the matcher
+  HostBuf h_qlisted;  // per-query listing counters, read after the matcher
+  HostOut hout[2];
+  int next_slot = 0;
+  uint64_t compactions = 0;
 
   // results (own lock: a waiter reads batch k while batch k + 1 runs)
   std::mutex rmu;
@@ -196,7 +239,7 @@ struct Engine {
   int upload_qd();
   int prepare_filters();
   int launch_filters();
-  int run_segment(int k, const std::function<int()> &fn);
+  int run_segment(int k, const std::string &key, const std::function<int()> &fn);
   int rec(cudaEvent_t ev);
   void elapsed(cudaEvent_t a, cudaEvent_t b, float *ms);
   bool capturing = false;
@@ -205,11 +248,31 @@ struct Engine {
   int query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);
 
   int check_updates(const dsm_update *ups, uint32_t n);
-  int autotune(MatchArgs &ma, unsigned long long seed_cap, size_t nseg, int &blocks);
+  int autotune(MatchArgs &ma, const Staged &S, int &blocks);
   int submit(const dsm_update *ups, uint32_t n, uint64_t *batch_id);
-  int run_batch(const dsm_update *ups, uint32_t n, BatchResult &R);
+  int graph_apply(const dsm_update *ups, uint32_t n);
+  // The batch pipeline (batch.cu): prepare (host only: sorted keys into the
+  // slot's pinned staging), launch_front (mu held: uploads, edge state, union
+  // insert, filters, seeds, matcher), finish_device (mu held: waits for the
+  // matcher, regrows and reruns on overflow, enqueues deletions and the
+  // downloads), assemble (host: waits for the downloads, builds the result).
+  // run_batch chains them; the serving loop overlaps assemble of batch k
+  // with the device work of batch k + 1.
+  int prepare(const dsm_update *ups, uint32_t n, Staged &S, int slot);
+  int launch_front(Staged &S);
+  int finish_device(Staged &S);
+  int assemble(Staged &S, BatchResult &R);
+  int run_batch(const dsm_update *ups, uint32_t n, BatchResult &R, bool match = true);
+  int run_front_and_finish(Staged &S);  // launch_front + finish_or_retry
+  int finish_or_retry(Staged &S);       // finish_device; on a refused batch, compact and run it again
+  int compact_arena(uint64_t extra_words);
+  int match_eager(Staged &S, MatchArgs &ma, SeedArgs &sa, int blocks);  // one launch, or one per query
+  int seg_a_kernels(Staged &S, const ClearArgs &ca, const EdgeStateArgs &es, const AdjUpdateArgs &au,
+                    const SeedArgs &sa, bool seeds);
+  std::mutex smu;  // stats written by assemble
   int wait_batch(uint64_t id);
-  void sort_segments(BatchResult &R, uint32_t nq_live, uint32_t n, size_t total);
+  void sort_segments(BatchResult &R, const std::vector<uint64_t> &counts, uint32_t nq_live, uint32_t n,
+                     size_t total);
   int view(uint64_t id, dsm_result_view *v);
   int release(uint64_t id);
   int timing(uint64_t id, dsm_batch_timing *t);
@@ -223,9 +286,10 @@ struct Engine {
   int admission(uint64_t ticket, int64_t timeout_ms, uint32_t *qid);
   void worker_loop();
   Outcome handle_control(Request &r);
+  void post_batch(struct InFlight &b);
+  void fail_batch(struct InFlight &b, int rc);
   void admit_pending();
   void post_outcome(uint64_t ticket, const Outcome &o);  // qmu held
-  void run_merged(std::vector<Request> &reqs);
 };
 
 }  // namespace dsm

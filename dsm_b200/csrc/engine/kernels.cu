@@ -39,15 +39,15 @@ __device__ void rebuild_loff(const DevGraph &g, uint32_t x, const uint32_t *run,
 // Edge state of a batch
 // ---------------------------------------------------------------------------
 __global__ void k_edge_state(EdgeStateArgs A) {
-  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= A.m) return;
+  const uint32_t M = A.hdr->m;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x) {
   unsigned long long key = A.bkey[j];
-  if (j > 0 && A.bkey[j - 1] == key) return;  // not a group head
+  if (j > 0 && A.bkey[j - 1] == key) continue;  // not a group head
   uint32_t a = (uint32_t)(key >> 32), b = (uint32_t)key;
   bool init = has_edge(A.g, a, b);
   bool state = init, inserted = false, any_change = false;
   uint32_t e = j;
-  for (; e < A.m && A.bkey[e] == key; ++e) {
+  for (; e < M && A.bkey[e] == key; ++e) {
     uint32_t i = A.bidx[e];
     uint32_t op = A.upd[i].x ? 1u : 0u;
     bool noop = op ? state : !state;
@@ -69,22 +69,23 @@ __global__ void k_edge_state(EdgeStateArgs A) {
     atomicOr(&A.g.lab[a], kTouchBit);
     atomicOr(&A.g.lab[b], kTouchBit);
   }
+  }
 }
 
-__device__ __forceinline__ uint8_t group_flag(const AdjUpdateArgs &A, uint32_t x, uint32_t y) {
+__device__ __forceinline__ uint8_t group_flag(const AdjUpdateArgs &A, uint32_t M, uint32_t x, uint32_t y) {
   unsigned long long key = canon_key(x, y);
-  uint32_t lo = 0, hi = A.m;
+  uint32_t lo = 0, hi = M;
   while (lo < hi) {
     uint32_t mid = (lo + hi) >> 1;
     if (A.bkey[mid] < key) lo = mid + 1; else hi = mid;
   }
-  return (lo < A.m && A.bkey[lo] == key) ? A.gflag[lo] : 0;
+  return (lo < M && A.bkey[lo] == key) ? A.gflag[lo] : 0;
 }
 
 // Compacts the entries of source group [s, e) selected by `want` (and, for
 // inserts, not yet in the run) into dsel[s..s+k), in entry order.  Returns k.
 // dkey holds x << 32 | entry of the neighbour, sorted.
-__device__ uint32_t select_group(const AdjUpdateArgs &A, uint32_t s, uint32_t e, uint32_t x,
+__device__ uint32_t select_group(const AdjUpdateArgs &A, uint32_t M, uint32_t s, uint32_t e, uint32_t x,
                                  uint8_t want, bool skip_present, const uint32_t *L, uint32_t d) {
   const uint32_t lane = threadIdx.x & 31;
   uint32_t k = 0;
@@ -96,7 +97,7 @@ __device__ uint32_t select_group(const AdjUpdateArgs &A, uint32_t s, uint32_t e,
       unsigned long long key = A.dkey[j];
       y = (uint32_t)key;
       bool first = (j == s) || (A.dkey[j - 1] != key);
-      sel = first && (group_flag(A, x, y & kIdMask) & want);
+      sel = first && (group_flag(A, M, x, y & kIdMask) & want);
       if (sel && skip_present) {
         uint32_t p = lower_bound_u32(L, d, y);
         sel = !(p < d && L[p] == y);
@@ -136,16 +137,54 @@ __device__ void merge_down(const uint32_t *L, uint32_t d, const uint32_t *N, uin
   }
 }
 
+// Arena units (16 bytes) the insert may take: per source group, the run's
+// new capacity when its degree plus every union insert of the group
+// outgrows the capacity it has.
+__global__ void k_arena_check(AdjUpdateArgs A) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t M = A.hdr->m, G = A.hdr->ngroups;
+  if (blockIdx.x == 0 && threadIdx.x == 0) A.need16[1] = *A.g.arena_top;
+  unsigned long long need = 0;
+  for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < G; gi += warps) {
+    const uint32_t s = A.dhead[gi], e = A.dhead[gi + 1];
+    const uint32_t x = (uint32_t)(A.dkey[s] >> 32);
+    uint32_t k = 0;
+    for (uint32_t base = s; base < e; base += 32) {
+      const uint32_t j = base + lane;
+      bool sel = false;
+      if (j < e) {
+        const unsigned long long key = A.dkey[j];
+        sel = (j == s || A.dkey[j - 1] != key) && (group_flag(A, M, x, (uint32_t)key & kIdMask) & 1u);
+      }
+      k += __popc(__ballot_sync(kFull, sel));
+    }
+    const uint32_t d = A.g.adj[x].y, c = A.g.cap[x];
+    if (lane == 0 && d + k > c) {
+      const uint32_t want = d + k;
+      need += ((want + want / 4 + 4 + 3) & ~3u) / 4;
+    }
+  }
+  if (lane == 0 && need) atomicAdd(&A.need16[0], need);
+}
+
 __global__ void k_adj_insert(AdjUpdateArgs A) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < A.ngroups; gi += warps) {
+  const uint32_t M = A.hdr->m, G = A.hdr->ngroups;
+  // all or nothing: every warp takes the same decision from the values the
+  // check left (the arena top as it was before this kernel)
+  if (A.need16[1] + A.need16[0] > A.g.arena_words / 4) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(A.err, kErrArena);
+    return;
+  }
+  for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < G; gi += warps) {
     uint32_t s = A.dhead[gi], e = A.dhead[gi + 1];
     uint32_t x = (uint32_t)(A.dkey[s] >> 32);
     uint2 ax = A.g.adj[x];
     uint32_t d = ax.y, c = A.g.cap[x];
     uint32_t *L = A.g.arena + (uint64_t)ax.x * 4;
-    uint32_t k = select_group(A, s, e, x, 1, true, L, d);
+    uint32_t k = select_group(A, M, s, e, x, 1, true, L, d);
     if (k == 0) continue;
     const uint32_t *N = A.dsel + s;
     if (d + k <= c) {
@@ -177,13 +216,15 @@ __global__ void k_adj_insert(AdjUpdateArgs A) {
 __global__ void k_adj_delete(AdjUpdateArgs A) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < A.ngroups; gi += warps) {
+  const uint32_t M = A.hdr->m, G = A.hdr->ngroups;
+  if (ld_volatile(*A.err) & kErrArena) return;  // the batch was refused: leave the graph as it was
+  for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < G; gi += warps) {
     uint32_t s = A.dhead[gi], e = A.dhead[gi + 1];
     uint32_t x = (uint32_t)(A.dkey[s] >> 32);
     uint2 ax = A.g.adj[x];
     uint32_t d = ax.y;
     uint32_t *L = A.g.arena + (uint64_t)ax.x * 4;
-    uint32_t k = select_group(A, s, e, x, 2, false, L, d);
+    uint32_t k = select_group(A, M, s, e, x, 2, false, L, d);
     if (k == 0) continue;
     const uint32_t *D = A.dsel + s;
     uint32_t removed = 0;
@@ -208,12 +249,36 @@ __global__ void k_adj_delete(AdjUpdateArgs A) {
   }
 }
 
-__global__ void k_clear_touch(DevGraph g, const uint4 *upd, uint32_t n) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint4 u = upd[i];
-  if (u.y < g.nv) atomicAnd(&g.lab[u.y], kLabelMask);
-  if (u.z < g.nv) atomicAnd(&g.lab[u.z], kLabelMask);
+__global__ void k_clear_touch(DevGraph g, const BatchHdr *hdr, const uint4 *upd) {
+  const uint32_t n = hdr->n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint4 u = upd[i];
+    if (u.y < g.nv) atomicAnd(&g.lab[u.y], kLabelMask);
+    if (u.z < g.nv) atomicAnd(&g.lab[u.z], kLabelMask);
+  }
+}
+
+__global__ void k_arena_move(DevGraph g, const uint2 *nadj, uint32_t *narena) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < g.nv; v += warps) {
+    const uint2 a = g.adj[v];
+    const uint32_t *src = g.arena + (uint64_t)a.x * 4;
+    uint32_t *dst = narena + (uint64_t)nadj[v].x * 4;
+    for (uint32_t i = lane; i < a.y; i += 32) dst[i] = src[i];
+  }
+}
+
+__global__ void k_batch_clear(ClearArgs A) {
+  const BatchHdr h = *A.hdr;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (size_t i = t; i < h.n; i += stride) A.vtp[i] = kNoView;
+  for (size_t i = t; i < h.nseg; i += stride) A.segcnt[i] = 0;
+  for (size_t i = t; i < h.nq_live; i += stride) A.qlisted[i] = 0;
+  uint32_t *sc = reinterpret_cast<uint32_t *>(A.sc);
+  for (size_t i = t; i < sizeof(Sched) / 4; i += stride) sc[i] = 0;
+  for (size_t i = t; i < 64; i += stride) A.misc[i] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -222,20 +287,22 @@ __global__ void k_clear_touch(DevGraph g, const uint4 *upd, uint32_t n) {
 // b in C(v).
 // ---------------------------------------------------------------------------
 __global__ void k_seeds(SeedArgs A) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
-  if (A.vtp[i] == kNoView) return;
+  const uint32_t n = A.hdr->n;
+  const unsigned long long seed_cap = A.hdr->seed_cap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  if (A.vtp[i] == kNoView) continue;
   uint4 u = A.upd[i];
   uint32_t a = u.y, b = u.z;
   // the engine validates updates on the host; callers that pass their own
   // device buffers (the allocation-free entry point) may not have: an id out
   // of range or a self loop seeds nothing
-  if (a >= A.g.nv || b >= A.g.nv || a == b) return;
+  if (a >= A.g.nv || b >= A.g.nv || a == b) continue;
   uint32_t la = A.g.lab[a] & kLabelMask, lb = A.g.lab[b] & kLabelMask;
-  if (la >= 32 || lb >= 32) return;
+  if (la >= 32 || lb >= 32) continue;
   uint32_t pb = la * 32 + lb;
   for (uint32_t e = A.pair_off[pb]; e < A.pair_off[pb + 1]; ++e) {
     uint32_t ent = A.pair_ent[e];
+    if (A.only_slot != kAllSlots && (ent >> 8) != A.only_slot) continue;
     const QDev &q = A.qd[ent >> 8];
     if (q.bitmap) {
       const OrderRec &o = A.orders[q.order_base + (ent & 255)];
@@ -244,37 +311,43 @@ __global__ void k_seeds(SeedArgs A) {
       if (!((q.bitmap[(size_t)qb * q.col_len + (b >> 5)] >> (b & 31)) & 1u)) continue;
     }
     unsigned long long s = atomicAdd(&A.sc->nseeds, 1ull);
-    if (s < A.seed_cap) A.seeds[s] = make_uint4(i, ent, a, b);
+    if (s < seed_cap) A.seeds[s] = make_uint4(i, ent, a, b);
+  }
   }
 }
 
 }  // namespace
 
-void launch_edge_state(const EdgeStateArgs &a, cudaStream_t s) {
-  if (a.m == 0) return;
-  k_edge_state<<<(a.m + 255) / 256, 256, 0, s>>>(a);
+void launch_batch_clear(const ClearArgs &a, int blocks, cudaStream_t s) {
+  k_batch_clear<<<blocks, 256, 0, s>>>(a);
 }
 
-void launch_adj_insert(const AdjUpdateArgs &a, cudaStream_t s) {
-  if (a.ngroups == 0) return;
-  uint32_t blocks = (a.ngroups + 7) / 8;
+void launch_edge_state(const EdgeStateArgs &a, int blocks, cudaStream_t s) {
+  k_edge_state<<<blocks, 256, 0, s>>>(a);
+}
+
+void launch_arena_check(const AdjUpdateArgs &a, int blocks, cudaStream_t s) {
+  k_arena_check<<<blocks, 256, 0, s>>>(a);
+}
+
+void launch_arena_move(DevGraph g, const uint2 *nadj, uint32_t *narena, int blocks, cudaStream_t s) {
+  k_arena_move<<<blocks, 256, 0, s>>>(g, nadj, narena);
+}
+
+void launch_adj_insert(const AdjUpdateArgs &a, int blocks, cudaStream_t s) {
   k_adj_insert<<<blocks, 256, 0, s>>>(a);
 }
 
-void launch_adj_delete(const AdjUpdateArgs &a, cudaStream_t s) {
-  if (a.ngroups == 0) return;
-  uint32_t blocks = (a.ngroups + 7) / 8;
+void launch_adj_delete(const AdjUpdateArgs &a, int blocks, cudaStream_t s) {
   k_adj_delete<<<blocks, 256, 0, s>>>(a);
 }
 
-void launch_clear_touch(DevGraph g, const uint4 *upd, uint32_t n, cudaStream_t s) {
-  if (n == 0) return;
-  k_clear_touch<<<(n + 255) / 256, 256, 0, s>>>(g, upd, n);
+void launch_clear_touch(DevGraph g, const BatchHdr *hdr, const uint4 *upd, int blocks, cudaStream_t s) {
+  k_clear_touch<<<blocks, 256, 0, s>>>(g, hdr, upd);
 }
 
-void launch_seeds(const SeedArgs &a, cudaStream_t s) {
-  if (a.n == 0) return;
-  k_seeds<<<(a.n + 255) / 256, 256, 0, s>>>(a);
+void launch_seeds(const SeedArgs &a, int blocks, cudaStream_t s) {
+  k_seeds<<<blocks, 256, 0, s>>>(a);
 }
 
 }  // namespace dsm

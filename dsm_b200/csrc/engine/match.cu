@@ -108,8 +108,8 @@ __device__ void finish_task(const MatchArgs &P) {
 // plain id-sorted runs.  srng[L][j]: for level L and backward neighbour j,
 // the range of j's run holding the label of level L (label-major only).
 template <bool kLM>
-__device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t depth, uint32_t lo,
-                         uint32_t hi, uint32_t fval, uint2 (*srng)[16]) {
+__device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t nupd, uint32_t upd, uint32_t qo,
+                         uint32_t depth, uint32_t lo, uint32_t hi, uint32_t fval, uint2 (*srng)[16]) {
   const uint32_t lane = threadIdx.x & 31;
   const QDev &Q = P.qd[qo >> 8];
   const uint32_t nq = Q.nq;
@@ -121,7 +121,7 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
   const uint32_t tp = P.vtp[upd];
   const uint32_t *bitmap = Q.bitmap;
   const uint32_t col_len = Q.col_len;
-  const uint32_t seg = Q.local * P.n + upd;
+  const uint32_t seg = Q.local * nupd + upd;
 
   uint32_t my_f = fval, my_off = 0, my_deg = 0, my_touch = 0;
   if (lane < depth) {
@@ -132,16 +132,23 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
   }
   unsigned long long alg = 0, task_cnt = 0;
 
-  // last level: the chunk's candidates are embeddings
+  // last level: the chunk's candidates are embeddings.  Listing reserves
+  // slots in the result table; a query past its listing budget reserves none
+  // (its count stays exact, the host drops its partial tuples).
   auto emit = [&](uint32_t m, uint32_t w, uint32_t L) {
     uint32_t cnt = __popc(m);
     if (cnt == 0) return;
     task_cnt += cnt;
     if (!P.list) return;
-    alg += 4ull * (nq + 1) * cnt;  // the tuple and its segment id
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(&P.sc->out_count.v, (unsigned long long)cnt);
+    unsigned long long base = ~0ull;
+    if (lane == 0) {
+      bool ok = true;
+      if (P.qlimit) ok = atomicAdd(&P.qlisted[Q.local], (unsigned long long)cnt) + cnt <= P.qlimit;
+      if (ok) base = atomicAdd(&P.sc->out_count.v, (unsigned long long)cnt);
+    }
     base = __shfl_sync(kFull, base, 0);
+    if (base == ~0ull) return;
+    alg += 4ull * (nq + 1) * cnt;  // the tuple and its segment id
     bool mine = (m >> lane) & 1u;
     unsigned long long s = base + __popc(m & lanemask_lt());
     bool wr = mine && s < P.cap;
@@ -157,7 +164,7 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
     if (lane == 0) {
       if (task_cnt) {
         atomicAdd(&P.seg_count[seg], task_cnt);
-        if (!P.list) atomicAdd(&P.sc->out_count.v, task_cnt);
+        atomicAdd(&P.sc->matches, task_cnt);
       }
       atomicAdd(&P.sc->alg_bytes, alg);
     }
@@ -278,7 +285,7 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
           uint32_t j = __ffs(bits) - 1;
           bits &= bits - 1;
           uint32_t fj = __shfl_sync(kFull, my_f, j), tj = __shfl_sync(kFull, my_touch, j);
-          if (ok && (lw >> 31) && tj) ok = edge_live(P.bt, fj, w, tp);
+          if (ok && (lw >> 31) && tj) ok = edge_live(bt, fj, w, tp);
         }
       }
       uint32_t m = __ballot_sync(kFull, ok);
@@ -422,9 +429,10 @@ __device__ void run_task(const MatchArgs &P, uint32_t upd, uint32_t qo, uint32_t
 
 // phantom = 1 adds one outstanding task that nothing finishes (a test of the
 // bounded waits: the launch then ends only through their timeouts).
-__global__ void k_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long long *job_seq,
-                             uint32_t job_ring, uint32_t phantom) {
+__global__ void k_sched_init(Sched *sc, const BatchHdr *hdr, unsigned long long *job_seq, uint32_t job_ring,
+                             uint32_t phantom) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long seed_cap = hdr->seed_cap;
   for (uint32_t s = i; s < job_ring; s += gridDim.x * blockDim.x) job_seq[s] = s;
   if (i == 0) {
     unsigned long long n = sc->nseeds;
@@ -446,6 +454,9 @@ template <bool kLM>
 __global__ void __launch_bounds__(256, DSM_MATCH_MIN_BLOCKS) k_match(MatchArgs P) {
   __shared__ uint2 s_rng[kLM ? 8 : 1][16][16];
   const uint32_t lane = threadIdx.x & 31;
+  if (*P.abort_flag & kErrArena) return;  // the batch was refused before its insert
+  const uint32_t nupd = P.hdr->n;
+  const DevBatchEdges bt{P.bt.bkey, P.bt.binfo, P.hdr->m};
   bool seeds_done = false;
   while (true) {
     uint32_t kind = 0;
@@ -476,16 +487,16 @@ __global__ void __launch_bounds__(256, DSM_MATCH_MIN_BLOCKS) k_match(MatchArgs P
       hi = __shfl_sync(kFull, word, 4);
       fval = __shfl_sync(kFull, word, (lane + 8) & 31);
     }
-    run_task<kLM>(P, upd, qo, depth, lo, hi, fval, s_rng[kLM ? (threadIdx.x >> 5) : 0]);
+    run_task<kLM>(P, bt, nupd, upd, qo, depth, lo, hi, fval, s_rng[kLM ? (threadIdx.x >> 5) : 0]);
     finish_task(P);
   }
 }
 
 }  // namespace
 
-void launch_sched_init(Sched *sc, unsigned long long seed_cap, unsigned long long *job_seq, uint32_t job_ring,
+void launch_sched_init(Sched *sc, const BatchHdr *hdr, unsigned long long *job_seq, uint32_t job_ring,
                        cudaStream_t s, uint32_t phantom) {
-  k_sched_init<<<(job_ring + 255) / 256, 256, 0, s>>>(sc, seed_cap, job_seq, job_ring, phantom);
+  k_sched_init<<<(job_ring + 255) / 256, 256, 0, s>>>(sc, hdr, job_seq, job_ring, phantom);
 }
 
 void launch_match(const MatchArgs &a, int blocks, cudaStream_t s) {

@@ -46,7 +46,8 @@ constexpr size_t kOffOrders = align256(kOffQd + sizeof(QDev));
 constexpr size_t kOffPairOff = align256(kOffOrders + sizeof(OrderRec) * kNaMaxOrders);
 constexpr size_t kOffPairEnt = align256(kOffPairOff + 4 * (32 * 32 + 1));
 constexpr size_t kOffVtp = align256(kOffPairEnt + 4 * kNaMaxOrders);
-constexpr size_t kScratchBytes = align256(kOffVtp + 4 * (size_t)kNaMaxUpdates);
+constexpr size_t kOffHdr = align256(kOffVtp + 4 * (size_t)kNaMaxUpdates);  // BatchHdr, then a zero word
+constexpr size_t kScratchBytes = align256(kOffHdr + sizeof(BatchHdr) + 16);
 
 static __device__ __align__(256) unsigned char g_na_scratch[kScratchBytes];
 
@@ -133,7 +134,15 @@ extern "C" int dsm_count_edge_embeddings_noalloc(int device, uint32_t nv, const 
   Sched *sc = (Sched *)(base + kOffSched);
   unsigned long long *seq = (unsigned long long *)(base + kOffSeq);
   uint32_t *vtp = (uint32_t *)(base + kOffVtp);
+  BatchHdr hdr;
+  std::memset(&hdr, 0, sizeof(hdr));
+  hdr.n = n;
+  hdr.nq_live = 1;
+  hdr.seed_cap = kNaSeedCap;
+  hdr.nseg = n;
   bool ok = cudaMemsetAsync(sc, 0, sizeof(Sched), s) == cudaSuccess &&
+            cudaMemcpyAsync(base + kOffHdr, &hdr, sizeof(hdr), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemsetAsync(base + kOffHdr + sizeof(BatchHdr), 0, 16, s) == cudaSuccess &&
             cudaMemcpyAsync(base + kOffQd, &qd, sizeof(qd), cudaMemcpyHostToDevice, s) == cudaSuccess &&
             cudaMemcpyAsync(base + kOffOrders, plan.orders.data(), plan.orders.size() * sizeof(OrderRec),
                             cudaMemcpyHostToDevice, s) == cudaSuccess &&
@@ -153,21 +162,23 @@ extern "C" int dsm_count_edge_embeddings_noalloc(int device, uint32_t nv, const 
   g.adj = reinterpret_cast<uint2 *>(const_cast<uint32_t *>(d_adj));
   g.arena = const_cast<uint32_t *>(d_arena);
 
-  SeedArgs sa{g, reinterpret_cast<const uint4 *>(d_updates), vtp, n, (const uint32_t *)(base + kOffPairOff),
+  const BatchHdr *dh = (const BatchHdr *)(base + kOffHdr);
+  SeedArgs sa{g, dh, reinterpret_cast<const uint4 *>(d_updates), vtp, (const uint32_t *)(base + kOffPairOff),
               (const uint32_t *)(base + kOffPairEnt), (const QDev *)(base + kOffQd),
-              (const OrderRec *)(base + kOffOrders), (uint4 *)(base + kOffSeeds), kNaSeedCap, sc};
-  launch_seeds(sa, s);
-  launch_sched_init(sc, kNaSeedCap, seq, kNaRing, s);
-
+              (const OrderRec *)(base + kOffOrders), (uint4 *)(base + kOffSeeds), sc, kAllSlots};
   int sms = 0, clk_khz = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, device);
+  launch_seeds(sa, std::max(sms, 1) * 4, s);
+  launch_sched_init(sc, dh, seq, kNaRing, s);
+
   MatchArgs ma;
   std::memset(&ma, 0, sizeof(ma));
   ma.g = g;
   ma.bt = DevBatchEdges{nullptr, nullptr, 0};  // a fixed graph: every edge is live
   ma.vtp = vtp;
-  ma.n = n;
+  ma.hdr = dh;
+  ma.abort_flag = (const unsigned int *)(base + kOffHdr + sizeof(BatchHdr));
   ma.qd = (const QDev *)(base + kOffQd);
   ma.orders = (const OrderRec *)(base + kOffOrders);
   ma.seeds = (const uint4 *)(base + kOffSeeds);

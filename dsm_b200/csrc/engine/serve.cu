@@ -161,75 +161,117 @@ Outcome Engine::handle_control(Request &r) {
   return o;
 }
 
+// The worker overlaps host and device work: while the device runs batch
+// k + 1 (its union insert, filters and matcher), the host assembles batch
+// k's results (copies, canonical sort) and hands them out.  A device batch's
+// host preparation (key sorting) happens as the previous batch's deletions
+// finish.  Control requests wait until the batch in flight is assembled.
+struct InFlight {
+  bool live = false;
+  std::vector<Request> reqs;
+  std::vector<dsm_update> all;
+  std::vector<uint32_t> start;
+  Staged S;
+  std::chrono::steady_clock::time_point t0;
+};
+
 void Engine::worker_loop() {
   cudaSetDevice(device);
+  InFlight cur, prev;
+  int slot = 0;
   std::unique_lock<std::mutex> q(srv.qmu);
   for (;;) {
+    if (prev.live && srv.queue.empty()) {  // nothing to overlap with: hand the last batch out
+      q.unlock();
+      post_batch(prev);
+      q.lock();
+      continue;
+    }
     srv.work_cv.wait(q, [&] { return !srv.queue.empty() || srv.stopping; });
     if (srv.queue.empty()) break;  // stopping, and everything queued was served
     if (srv.queue.front().kind != kReqBatch) {
       Request r = std::move(srv.queue.front());
       srv.queue.pop_front();
       q.unlock();
+      if (prev.live) post_batch(prev);
       Outcome o = handle_control(r);
       q.lock();
       if (o.rc != -1) post_outcome(r.id, o);
       srv.done_cv.notify_all();
       continue;
     }
-    std::vector<Request> reqs;
+    cur = InFlight();
     size_t total = 0;
     while (!srv.queue.empty() && srv.queue.front().kind == kReqBatch &&
-           (reqs.empty() || total + srv.queue.front().ups.size() <= srv.max_merge)) {
+           (cur.reqs.empty() || total + srv.queue.front().ups.size() <= srv.max_merge)) {
       total += srv.queue.front().ups.size();
-      reqs.push_back(std::move(srv.queue.front()));
+      cur.reqs.push_back(std::move(srv.queue.front()));
       srv.queue.pop_front();
     }
     q.unlock();
-    run_merged(reqs);
+    cur.start.assign(cur.reqs.size() + 1, 0);
+    for (size_t k = 0; k < cur.reqs.size(); ++k) {
+      cur.all.insert(cur.all.end(), cur.reqs[k].ups.begin(), cur.reqs[k].ups.end());
+      cur.start[k + 1] = (uint32_t)cur.all.size();
+    }
+    cur.live = true;
+    slot ^= 1;
+    int rc;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      cur.t0 = std::chrono::steady_clock::now();
+      cudaSetDevice(device);
+      rc = prepare(cur.all.data(), (uint32_t)cur.all.size(), cur.S, slot);
+      if (!rc) rc = launch_front(cur.S);
+    }
+    if (prev.live) post_batch(prev);  // host work of batch k while the device runs batch k + 1
+    if (!rc) {
+      std::lock_guard<std::mutex> lk(mu);
+      rc = finish_or_retry(cur.S);
+    }
+    if (rc) {
+      fail_batch(cur, rc);
+    } else {
+      prev = std::move(cur);
+    }
     q.lock();
     srv.done_cv.notify_all();
   }
+  q.unlock();
+  if (prev.live) post_batch(prev);
 }
 
-// One device batch for consecutive batch requests; each request gets its own
-// result (its updates' slice of every per-(query, update) array).
-void Engine::run_merged(std::vector<Request> &reqs) {
-  std::vector<dsm_update> all;
-  std::vector<uint32_t> start(reqs.size() + 1, 0);
-  for (size_t k = 0; k < reqs.size(); ++k) {
-    all.insert(all.end(), reqs[k].ups.begin(), reqs[k].ups.end());
-    start[k + 1] = (uint32_t)all.size();
+void Engine::fail_batch(InFlight &b, int rc) {
+  const std::string msg = error_text();
+  std::lock_guard<std::mutex> q(srv.qmu);
+  for (Request &r : b.reqs) {
+    srv.failed[r.id] = Outcome{rc, 0, msg};
+    srv.inflight.erase(r.id);
   }
-  const uint32_t N = (uint32_t)all.size();
+  b.live = false;
+  srv.done_cv.notify_all();
+}
+
+// Assembles an in-flight device batch and gives each request its own result
+// (its updates' slice of every per-(query, update) array).
+void Engine::post_batch(InFlight &b) {
   BatchResult R;
-  int rc;
-  std::string msg;
-  std::chrono::steady_clock::time_point t0;
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    t0 = std::chrono::steady_clock::now();
-    cudaSetDevice(device);
-    rc = run_batch(all.data(), N, R);
-    if (rc) msg = error_text();
-  }
+  const int rc = assemble(b.S, R);
   if (rc) {
-    std::lock_guard<std::mutex> q(srv.qmu);
-    for (Request &r : reqs) {
-      srv.failed[r.id] = Outcome{rc, 0, msg};
-      srv.inflight.erase(r.id);
-    }
+    fail_batch(b, rc);
     return;
   }
+  const uint32_t N = (uint32_t)b.all.size();
   const uint32_t nql = (uint32_t)R.qids.size();
   std::vector<std::unique_ptr<BatchResult>> outs;
-  for (size_t k = 0; k < reqs.size(); ++k) {
-    const uint32_t s = start[k], n = start[k + 1] - s;
+  for (size_t k = 0; k < b.reqs.size(); ++k) {
+    const uint32_t s = b.start[k], n = b.start[k + 1] - s;
     auto o = std::make_unique<BatchResult>();
-    o->id = reqs[k].id;
+    o->id = b.reqs[k].id;
     o->n = n;
     o->qids = R.qids;
     o->widths = R.widths;
+    o->qlisted = R.qlisted;
     o->listed = R.listed;
     o->signs.assign(R.signs.begin() + s, R.signs.begin() + s + n);
     o->counts.resize((size_t)nql * n);
@@ -243,28 +285,30 @@ void Engine::run_merged(std::vector<Request> &reqs) {
     if (R.listed) {
       o->tuples.resize(o->offsets.back());
       for (uint32_t ql = 0; ql < nql; ++ql) {  // each query's slice is contiguous
-        const size_t a = R.offsets[(size_t)ql * N + s], b = R.offsets[(size_t)ql * N + s + n];
-        std::copy(R.tuples.begin() + a, R.tuples.begin() + b, o->tuples.begin() + o->offsets[(size_t)ql * n]);
+        const size_t a = R.offsets[(size_t)ql * N + s], e = R.offsets[(size_t)ql * N + s + n];
+        std::copy(R.tuples.begin() + a, R.tuples.begin() + e, o->tuples.begin() + o->offsets[(size_t)ql * n]);
       }
     }
     o->device_ms = R.device_ms;
     o->match_ms = R.match_ms;
-    o->merged_requests = (uint32_t)reqs.size();
+    o->merged_requests = (uint32_t)b.reqs.size();
     o->merged_updates = N;
     outs.push_back(std::move(o));
   }
   const auto t1 = std::chrono::steady_clock::now();
   {
     std::lock_guard<std::mutex> r(rmu);
-    for (size_t k = 0; k < reqs.size(); ++k) {
-      outs[k]->queue_ms = ms_between(reqs[k].t_submit, t0);
-      outs[k]->service_ms = ms_between(t0, t1);
-      outs[k]->total_ms = ms_between(reqs[k].t_submit, t1);
-      results[reqs[k].id] = std::move(outs[k]);
+    for (size_t k = 0; k < b.reqs.size(); ++k) {
+      outs[k]->queue_ms = ms_between(b.reqs[k].t_submit, b.t0);
+      outs[k]->service_ms = ms_between(b.t0, t1);
+      outs[k]->total_ms = ms_between(b.reqs[k].t_submit, t1);
+      results[b.reqs[k].id] = std::move(outs[k]);
     }
   }
   std::lock_guard<std::mutex> q(srv.qmu);
-  for (Request &r : reqs) srv.inflight.erase(r.id);
+  for (Request &r : b.reqs) srv.inflight.erase(r.id);
+  b.live = false;
+  srv.done_cv.notify_all();
 }
 
 }  // namespace dsm

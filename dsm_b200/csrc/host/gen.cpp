@@ -9,6 +9,7 @@
 // Determinism: std::mt19937_64 streams with hand-written samplers (no
 // std::*_distribution, whose output differs between standard libraries).
 #include "dsm_host.h"
+#include "par.h"
 
 #include <algorithm>
 #include <atomic>
@@ -56,21 +57,33 @@ uint32_t sample_cdf(const std::vector<double> &cdf, Rng &r) {
 }
 
 // Distinct undirected edges without self loops until `m` are found, then a
-// seeded shuffle fixes their order.
+// seeded shuffle fixes their order.  Each round draws in fixed chunks of 2^20
+// edges, chunk c with its own generator seeded from the round's seed and c,
+// so the chunks run on all host threads and the result does not depend on
+// the thread count.
 template <class Draw>
 std::vector<uint64_t> distinct_edges(uint64_t m, Rng &r, Draw draw) {
   std::vector<uint64_t> keys;
   keys.reserve(m + m / 4);
+  constexpr size_t kGrain = 1u << 20;
   while (keys.size() < m) {
-    uint64_t need = m - keys.size();
-    uint64_t batch = need + need / 8 + 1024;
-    for (uint64_t k = 0; k < batch; ++k) {
-      uint32_t a, b;
-      draw(a, b);
-      if (a == b) continue;
-      keys.push_back(edge_key(a, b));
-    }
-    std::sort(keys.begin(), keys.end());
+    const uint64_t need = m - keys.size();
+    const uint64_t batch = need + need / 8 + 1024;
+    const uint64_t round_seed = r.u64();
+    const size_t nchunks = (batch + kGrain - 1) / kGrain;
+    std::vector<std::vector<uint64_t>> part(nchunks);
+    parallel_chunks(nchunks, [&](size_t c) {
+      Rng rc(round_seed ^ (0x9E3779B97F4A7C15ull * (c + 1)));
+      const uint64_t lo = c * kGrain, hi = std::min<uint64_t>(batch, lo + kGrain);
+      part[c].reserve(hi - lo);
+      for (uint64_t k = lo; k < hi; ++k) {
+        uint32_t a, b;
+        draw(rc, a, b);
+        if (a != b) part[c].push_back(edge_key(a, b));
+      }
+    });
+    for (auto &pc : part) keys.insert(keys.end(), pc.begin(), pc.end());
+    parallel_sort(keys);
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
   }
   shuffle(keys, r);
@@ -82,16 +95,18 @@ void relabel_ids(std::vector<uint64_t> &keys, uint32_t nv, Rng &r) {
   std::vector<uint32_t> perm(nv);
   for (uint32_t i = 0; i < nv; ++i) perm[i] = i;
   shuffle(perm, r);
-  for (auto &k : keys) k = edge_key(perm[k >> 32], perm[(uint32_t)k]);
+  parallel_for(keys.size(), 1u << 20, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) keys[i] = edge_key(perm[keys[i] >> 32], perm[(uint32_t)keys[i]]);
+  });
 }
 
 std::vector<uint64_t> gen_rmat(uint32_t log2_nv, uint64_t m, double a, double b, double c,
                                Rng &r) {
   const double ab = a + b, abc = a + b + c;
-  auto draw = [&](uint32_t &s, uint32_t &d) {
+  auto draw = [&](Rng &rr, uint32_t &s, uint32_t &d) {
     s = d = 0;
     for (uint32_t l = 0; l < log2_nv; ++l) {
-      double x = r.unit();
+      double x = rr.unit();
       uint32_t bs = 0, bd = 0;
       if (x < a) {
       } else if (x < ab) {
@@ -125,9 +140,9 @@ std::vector<uint64_t> gen_chung_lu(uint32_t nv, uint64_t m, double gamma, Rng &r
     acc += std::min(w[i] * scale, cap);
     cdf[i] = acc;
   }
-  auto draw = [&](uint32_t &s, uint32_t &d) {
-    s = sample_cdf(cdf, r);
-    d = sample_cdf(cdf, r);
+  auto draw = [&](Rng &rr, uint32_t &s, uint32_t &d) {
+    s = sample_cdf(cdf, rr);
+    d = sample_cdf(cdf, rr);
   };
   auto keys = distinct_edges(m, r, draw);
   relabel_ids(keys, nv, r);
@@ -171,7 +186,9 @@ Adj build_adj(uint32_t nv, const std::vector<uint64_t> &keys) {
     g.nbr[pos[a]++] = b;
     g.nbr[pos[b]++] = a;
   }
-  for (uint32_t v = 0; v < nv; ++v) std::sort(g.nbr.begin() + g.off[v], g.nbr.begin() + g.off[v + 1]);
+  parallel_for(nv, 1u << 14, [&](size_t lo, size_t hi) {
+    for (size_t v = lo; v < hi; ++v) std::sort(g.nbr.begin() + g.off[v], g.nbr.begin() + g.off[v + 1]);
+  });
   return g;
 }
 

@@ -90,6 +90,14 @@ const char *dsm_last_error(dsm_engine *e);
                                    (DSM_OPT_TIMEOUT_MS without progress) and the batch returns
                                    DSM_ERR_TIMEOUT after applying its updates to the graph.
                                    Tests the failure path without faulting the device. */
+#define DSM_OPT_PLAIN 16        /* 1: each batch runs the matcher once per registered query, in
+                                   turn, with a host round trip after each launch -- the
+                                   reference's one-query-per-process form, kept as the baseline
+                                   of the batched form; results identical (default 0) */
+#define DSM_OPT_QUERY_LIST_LIMIT 17 /* tuples one query may list in one batch (0: no limit,
+                                   the default).  A query over it is reported with exact
+                                   counts and no tuples for that batch (query_listed = 0 in
+                                   the view); the other queries stay listed. */
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
 int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
 
@@ -108,6 +116,11 @@ int dsm_graph_load_edges(dsm_engine *e, uint32_t nv, const uint32_t *labels, uin
  * (cpuGraph.cpp:521-607): the device lists must equal the set rebuild. */
 int dsm_graph_export(dsm_engine *e, uint32_t *offsets, uint32_t *nbrs, uint64_t *num_entries);
 int dsm_graph_info(dsm_engine *e, uint32_t *nv, uint64_t *num_entries, uint64_t *arena_words);
+/* Applies a batch of updates to the device graph without matching, in array
+ * order with set semantics -- updateHostGraph (cpuGraph.cpp:521-607) plus the
+ * re-upload of copyGraphToGPU (io.cu:254-302), as one device step.  Not
+ * available while the serving loop runs (DSM_ERR_STATE). */
+int dsm_graph_apply(dsm_engine *e, const dsm_update *ups, uint32_t n);
 
 /* ---- queries ---------------------------------------------------------- */
 /* Query CSR as read from a query file (file order, io.cu:181-189).  The
@@ -164,7 +177,10 @@ typedef struct dsm_result_view {
   const uint64_t *counts;   /* [num_queries * num_updates], query-major */
   const uint64_t *offsets;  /* [num_queries * num_updates + 1]: word offsets into tuples */
   const uint32_t *tuples;   /* (f(0)..f(nq-1)) per embedding, each segment sorted */
-  int listed;               /* 0 when the batch ran with DSM_OPT_LIST = 0 */
+  int listed;               /* 0 when the batch ran with DSM_OPT_LIST = 0 (or over the
+                               batch listing limit): counts only */
+  const uint8_t *query_listed; /* [num_queries]: 1 when that query's tuples are listed
+                               (0 past DSM_OPT_QUERY_LIST_LIMIT: its segments are empty) */
 } dsm_result_view;
 /* Waits if needed; the view stays valid until dsm_batch_release. */
 int dsm_batch_results(dsm_engine *e, uint64_t batch_id, dsm_result_view *view);
@@ -285,7 +301,9 @@ typedef struct dsm_stats {
   uint64_t tune_runs;        /* matcher launches timed by the autotuner */
   double tune_best_ms;       /* the fastest of them (last tuning) */
   uint64_t graph_launches;   /* segment graphs launched (DSM_OPT_GRAPH) */
-  uint64_t graph_instantiations; /* of which needed a new executable graph */
+  uint64_t graph_instantiations; /* executable graphs instantiated */
+  uint64_t graph_captures;   /* segments captured (a replay reuses the last capture) */
+  uint64_t compactions;      /* adjacency arena compactions */
 } dsm_stats;
 int dsm_engine_stats(dsm_engine *e, dsm_stats *s);
 

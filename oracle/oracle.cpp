@@ -1110,6 +1110,50 @@ int orc_stream_apply_graph(orc_stream *h, uint32_t n, const uint32_t *ups) {
   return 0;
 }
 
+int orc_stream_set_query(orc_stream *h, uint32_t nq, const uint32_t *qlabels, const uint32_t *qoff,
+                         const uint32_t *qnbr) {
+  if (nq < 2 || nq > 16) return -2;
+  Stream &S = h->s;
+  std::vector<Stream::Seed> seeds;
+  for (uint32_t u = 0; u < nq; ++u)
+    for (uint32_t k = qoff[u]; k < qoff[u + 1]; ++k) {
+      Stream::Seed sd;
+      sd.u = u;
+      sd.v = qnbr[k];
+      order_impl(nq, qoff, qnbr, sd.u, sd.v, sd.order, sd.bn);
+      if (sd.order.size() != nq) return -1;
+      seeds.push_back(sd);
+    }
+  S.nq = nq;
+  S.qlabels.assign(qlabels, qlabels + nq);
+  S.qoff.assign(qoff, qoff + nq + 1);
+  S.qnbr.assign(qnbr, qnbr + qoff[nq]);
+  S.seeds.swap(seeds);
+  return 0;
+}
+
+uint64_t orc_stream_probe(orc_stream *h, uint32_t op, uint32_t a, uint32_t b, int threads) {
+  Stream &S = h->s;
+  if (a >= S.nv || b >= S.nv || a == b) return 0;
+  if (threads < 1) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  const bool present = S.has_edge(a, b);
+  if (op == 1 && present) return 0;
+  if (op != 1 && !present) return 0;
+  auto &la = S.adj[a], &lb = S.adj[b];
+  if (op == 1) {
+    la.insert(std::lower_bound(la.begin(), la.end(), b), b);
+    lb.insert(std::lower_bound(lb.begin(), lb.end(), a), a);
+  }
+  Pool pool(threads);
+  std::vector<uint32_t> none;
+  const uint64_t c = match_edge_mt(S, a, b, false, none, pool, threads);
+  if (op == 1) {
+    la.erase(std::lower_bound(la.begin(), la.end(), b));
+    lb.erase(std::lower_bound(lb.begin(), lb.end(), a));
+  }
+  return c;
+}
+
 void orc_stream_set_budget(orc_stream *h, uint64_t bytes) { h->s.work_budget = bytes; }
 uint32_t orc_stream_complete(const orc_stream *h) { return h->s.complete; }
 

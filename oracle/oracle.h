@@ -106,6 +106,13 @@ void orc_stream_set_budget(orc_stream *s, uint64_t bytes);
  * results; updates apply in order, each update's search is shared among the
  * threads.  No work budget. */
 int orc_stream_apply_mt(orc_stream *s, uint32_t n, const uint32_t *updates, int list, int threads);
+/* Replaces the stream's query (the graph stays): one graph, many queries. */
+int orc_stream_set_query(orc_stream *s, uint32_t nq, const uint32_t *qlabels, const uint32_t *qoff,
+                         const uint32_t *qnbr);
+/* The count update (op, a, b) would report if it were applied now (on
+ * `threads` host threads, < 1: all cores); the graph is left unchanged.  An
+ * insert of a present edge, a delete of an absent one or a self loop: 0. */
+uint64_t orc_stream_probe(orc_stream *s, uint32_t op, uint32_t a, uint32_t b, int threads);
 /* Applies the updates to the graph only (no matching). */
 int orc_stream_apply_graph(orc_stream *s, uint32_t n, const uint32_t *updates);
 uint32_t orc_stream_complete(const orc_stream *s);

@@ -44,6 +44,8 @@ _sig("orc_stream_free", None, P)
 _sig("orc_stream_apply", C.c_int, P, C.c_uint32, u32p, C.c_int)
 _sig("orc_stream_apply_mt", C.c_int, P, C.c_uint32, u32p, C.c_int, C.c_int)
 _sig("orc_stream_apply_graph", C.c_int, P, C.c_uint32, u32p)
+_sig("orc_stream_set_query", C.c_int, P, C.c_uint32, u32p, u32p, u32p)
+_sig("orc_stream_probe", C.c_uint64, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int)
 _sig("orc_stream_set_budget", None, P, C.c_uint64)
 _sig("orc_stream_complete", C.c_uint32, P)
 _sig("orc_stream_sign", C.c_int8, P, C.c_uint32)
@@ -52,6 +54,16 @@ _sig("orc_stream_tuples", C.POINTER(C.c_uint32), P, C.POINTER(C.c_uint64))
 _sig("orc_stream_count_all", C.c_uint64, P)
 _sig("orc_stream_export", C.c_uint64, P, P, P)
 _sig("orc_stream_bytes", C.c_uint64, P)
+_sig("orc_workload_generate", C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_uint32, C.POINTER(P))
+_sig("orc_workload_free", None, P)
+for n in ("nv", "num_queries", "num_batches", "num_updates"):
+    _sig(f"orc_workload_{n}", C.c_uint32, P)
+_sig("orc_workload_num_edges", C.c_uint64, P)
+for n in ("labels", "edges", "batch_sizes", "updates"):
+    _sig(f"orc_workload_{n}", C.POINTER(C.c_uint32), P)
+_sig("orc_workload_query_nv", C.c_uint32, P, C.c_uint32)
+for n in ("labels", "offsets", "nbrs"):
+    _sig(f"orc_workload_query_{n}", C.POINTER(C.c_uint32), P, C.c_uint32)
 _sig("orc_bruteforce_count", C.c_uint64, C.c_uint32, u32p, u32p, u32p, C.c_uint32, u32p, u32p, u32p)
 
 
@@ -180,6 +192,16 @@ class Stream:
         if len(u) and lib.orc_stream_apply_graph(self._h, len(u) // 4, u):
             raise ValueError("oracle apply failed")
 
+    def set_query(self, qlabels, qoff, qnbr):
+        """Replaces the query; the graph stays."""
+        if lib.orc_stream_set_query(self._h, len(qlabels), _u32(qlabels), _u32(qoff), _u32(qnbr)):
+            raise ValueError("oracle: bad query")
+        self.nq = len(qlabels)
+
+    def probe(self, op, a, b, threads=-1):
+        """Count update (op, a, b) would report now; the graph is unchanged."""
+        return lib.orc_stream_probe(self._h, int(op), int(a), int(b), int(threads))
+
     def set_budget(self, nbytes):
         """Work budget (algorithmic bytes) of each later apply call."""
         lib.orc_stream_set_budget(self._h, int(nbytes))
@@ -204,3 +226,43 @@ def bruteforce_count(qlabels, qoff, qnbr, nv, labels, off, nbr):
         nbr = np.zeros(1, np.uint32)
     return lib.orc_bruteforce_count(len(qlabels), _u32(qlabels), _u32(qoff), _u32(qnbr), nv, _u32(labels),
                                     _u32(off), nbr)
+
+
+class Query:
+    def __init__(self, labels, offsets, nbrs):
+        self.labels, self.offsets, self.nbrs = _u32(labels), _u32(offsets), _u32(nbrs)
+
+    @property
+    def nv(self):
+        return len(self.labels)
+
+
+class Workload:
+    """The engine's seeded workload (same generator source, compiled into the
+    oracle library), for the CPU arms that must not load the engine."""
+
+    def __init__(self, config, seed=0, scale_log2=0, num_batches=0):
+        h = P()
+        if lib.orc_workload_generate(config, seed, scale_log2, num_batches, C.byref(h)):
+            raise ValueError("oracle: workload generation failed")
+        try:
+            self.nv = lib.orc_workload_nv(h)
+            self.labels = _arr(lib.orc_workload_labels(h), self.nv)
+            ne = lib.orc_workload_num_edges(h)
+            self.edges = _arr(lib.orc_workload_edges(h), 2 * ne).reshape(-1, 2)
+            self.queries = []
+            for q in range(lib.orc_workload_num_queries(h)):
+                nq = lib.orc_workload_query_nv(h, q)
+                off = _arr(lib.orc_workload_query_offsets(h, q), nq + 1)
+                self.queries.append(Query(_arr(lib.orc_workload_query_labels(h, q), nq), off,
+                                          _arr(lib.orc_workload_query_nbrs(h, q), int(off[-1]))))
+            self.batch_sizes = _arr(lib.orc_workload_batch_sizes(h), lib.orc_workload_num_batches(h))
+            self.updates = _arr(lib.orc_workload_updates(h), 4 * lib.orc_workload_num_updates(h)).reshape(-1, 4)
+        finally:
+            lib.orc_workload_free(h)
+
+    def batches(self):
+        pos = 0
+        for s in self.batch_sizes:
+            yield self.updates[pos:pos + int(s)]
+            pos += int(s)

@@ -1,0 +1,160 @@
+"""Engine paths beside the batched matcher, each against the oracle or the
+batched form: the plain form (one matcher launch per query, the reference's
+one-query-per-process loop), per-query listing budgets, graph-only apply,
+and the adjacency arena's compaction and all-or-nothing refusal."""
+import numpy as np
+import pytest
+
+import dsm_b200 as d
+from tests.helpers import compare_batch, oracle_apply, oracle_stream, run_stream
+
+pytestmark = pytest.mark.gpu
+OOM = 2
+
+
+def _fresh(nv, labels, edges, queries, **opts):
+    e = d.Engine(0)
+    for k, v in opts.items():
+        e.set_option(getattr(d, k), v)
+    e.load_graph_edges(nv, labels, edges)
+    return e, [e.register(q) for q in queries]
+
+
+def _same(ra, rb):
+    assert np.array_equal(ra.signs, rb.signs)
+    assert np.array_equal(ra.counts, rb.counts)
+    assert np.array_equal(ra.offsets, rb.offsets)
+    assert np.array_equal(ra.tuples, rb.tuples)
+
+
+def test_plain_form_equals_batched():
+    """32 config-3 queries (scaled graph): one launch per query per batch
+    gives the batched form's listed results, update by update."""
+    w = d.Workload(3, scale_log2=-6, num_batches=2)
+    bs = [b[:512] for b in w.batches()]
+    qs = w.queries[:32]
+    a, _ = _fresh(w.nv, w.labels, w.edges, qs)
+    p, qids = _fresh(w.nv, w.labels, w.edges, qs, OPT_PLAIN=1)
+    st = oracle_stream(w.nv, w.labels, w.edges, qs[0])
+    for b in bs:
+        ra, rp = a.run_batch(b), p.run_batch(b)
+        _same(ra, rp)
+        s, c, t, v = oracle_apply(st, b, listed=True, limit=200_000)
+        compare_batch(rp, qids[0], s, c, t, v, tag="plain form, query 0")
+    assert p.stats()["kernel_launches"] > a.stats()["kernel_launches"]
+    for x, y in zip(a.export_graph(), p.export_graph()):
+        assert np.array_equal(x, y)
+    a.close()
+    p.close()
+
+
+@pytest.mark.parametrize("plain", [0, 1])
+def test_query_list_limit_drops_only_heavy_queries(plain):
+    """With a per-query listing budget, a query that would list more in a
+    batch reports exact counts and no tuples; every other query is listed
+    exactly as without the budget."""
+    w = d.Workload(3, scale_log2=-6, num_batches=1)
+    b = next(w.batches())[:512]
+    qs = w.queries[:16]
+    full, _ = _fresh(w.nv, w.labels, w.edges, qs)
+    rf = full.run_batch(b)
+    per_q = rf.counts.sum(axis=1)
+    nz = np.sort(per_q[per_q > 0])
+    assert len(nz) >= 2
+    limit = int(nz[len(nz) // 2])  # about half of the non-empty queries go over
+    lim, _ = _fresh(w.nv, w.labels, w.edges, qs, OPT_QUERY_LIST_LIMIT=limit, OPT_PLAIN=plain)
+    rl = lim.run_batch(b)
+    assert np.array_equal(rf.counts, rl.counts)
+    want = per_q <= limit
+    assert np.array_equal(rl.query_listed, want)
+    assert (~want).any() and want.any()
+    for ql, qid in enumerate(rl.qids):
+        for i in range(len(b)):
+            t = rl.tuples_of(qid, i)
+            if want[ql]:
+                assert np.array_equal(t, rf.tuples_of(qid, i))
+            else:
+                assert len(t) == 0
+    full.close()
+    lim.close()
+
+
+def test_graph_apply_equals_oracle_and_matching_continues():
+    w = d.Workload(1)
+    q = w.queries[0]
+    e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
+    st = oracle_stream(w.nv, w.labels, w.edges, q)
+    ups = w.updates
+    e.apply_graph(ups[:2000])
+    st.apply_graph(ups[:2000])
+    for x, y in zip(e.export_graph(), st.export()):
+        assert np.array_equal(x, y)
+    r = e.run_batch(ups[2000:2600])
+    s, c, t, v = oracle_apply(st, ups[2000:2600], listed=True)
+    compare_batch(r, qid, s, c, t, v, tag="after graph apply")
+    e.close()
+
+
+def _insert_stream(w, nbatches, size, seed):
+    """Batches of inserts of absent edges (and a few deletes), enough to
+    outgrow the slack of many runs."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nbatches):
+        a = rng.integers(0, w.nv, size)
+        b = rng.integers(0, w.nv, size)
+        op = (rng.random(size) < 0.9).astype(np.uint32)
+        out.append(np.stack([op, a, b, np.zeros(size)], axis=1).astype(np.uint32))
+    return out
+
+
+def test_arena_compaction_long_insert_stream():
+    """A config-1 graph takes 16 batches of 4096 mostly-insert updates (its
+    edge count grows 3x): runs relocate, the arena compacts, and every batch
+    and the final graph equal the oracle."""
+    w = d.Workload(1)
+    q = w.queries[0]
+    e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
+    st = oracle_stream(w.nv, w.labels, w.edges, q)
+    bs = _insert_stream(w, 16, 4096, 5)
+    total, checked = run_stream(e, [qid], [st], bs, check_graph_every=4, limit=500_000)
+    s = e.stats()
+    assert s["compactions"] >= 1, s
+    assert s["relocations"] > 0
+    assert checked > 0
+    e.close()
+
+
+def test_arena_refusal_leaves_graph_unchanged():
+    """With the memory budget pinned to the bytes in use, a batch whose
+    relocations do not fit the arena is refused before it writes anything
+    (DSM_ERR_OOM, graph unchanged); with room it then runs and equals the
+    oracle."""
+    w = d.Workload(1)
+    q = w.queries[0]
+    e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q], OPT_LIST=0)  # counts: no result table to regrow
+    st = oracle_stream(w.nv, w.labels, w.edges, q)
+    bs = _insert_stream(w, 12, 4096, 9)
+    refused = None
+    for k, b in enumerate(bs):
+        if k == 1:  # every scratch buffer has its size: only the arena can run out now
+            e.set_option(d.OPT_MEM_BUDGET, e.stats()["device_bytes_in_use"])
+        before = e.export_graph()
+        try:
+            r = e.run_batch(b)
+        except d.DSMError as ex:
+            assert ex.code == OOM, str(ex)
+            after = e.export_graph()
+            assert all(np.array_equal(x, y) for x, y in zip(before, after)), "refused batch changed the graph"
+            refused = k
+            break
+        s, c, t, v = oracle_apply(st, b, listed=False, limit=500_000)
+        compare_batch(r, qid, s, c, t, v, tag=f"batch {k}")
+    assert refused is not None, "the arena never ran out"
+    e.set_option(d.OPT_MEM_BUDGET, 64 << 30)
+    r = e.run_batch(bs[refused])
+    s, c, t, v = oracle_apply(st, bs[refused], listed=False, limit=500_000)
+    compare_batch(r, qid, s, c, t, v, tag="refused batch, run again with room")
+    for x, y in zip(e.export_graph(), st.export()):
+        assert np.array_equal(x, y)
+    e.close()

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import dsm_b200 as d
-from helpers import compare_batch, oracle_apply, oracle_stream
+from tests.helpers import compare_batch, oracle_apply, oracle_stream
 
 pytestmark = pytest.mark.gpu
 

@@ -1,0 +1,109 @@
+"""Parity on the work the benchmark times, at full size.
+
+The budgeted oracle of the other parity tests skips the heaviest updates,
+which are the ones that dominate a timed batch.  Here the engine runs whole
+batches in count mode on full-size graphs, and for each query the oracle's
+all-cores matcher recounts the heaviest updates (up to a ceiling it finishes
+in seconds) and some random ones, each on exactly the graph state that update
+sees (the oracle's graph is advanced to just before it; `probe` counts the
+update without applying it).  Counts must be equal.
+
+- config 2 at full size: 2^20 vertices, 2^24 edges, the three 8-vertex
+  queries, one 4096-update batch;
+- config 3: 256 queries of 4-12 vertices on the full-size graph, one
+  512-update slice, all queries in one launch;
+- config 5 at 1/16 scale (2^18 vertices, 2^23 edges, hubs above 10^4): 64
+  twelve-vertex cyclic queries, one 65,536-update batch, 80 % deletions.
+"""
+import numpy as np
+import pytest
+
+import dsm_b200 as d
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine_counts(w, queries, batch):
+    e = d.Engine(0)
+    e.set_option(d.OPT_LIST, 0)
+    e.load_graph_edges(w.nv, w.labels, w.edges)
+    qids = [e.register(q) for q in queries]
+    r = e.run_batch(batch)
+    counts = np.stack([r.counts[r.query_index(q)] for q in qids])
+    signs = r.signs.copy()
+    st = e.stats()
+    e.close()
+    return counts, signs, st
+
+
+def _pick(counts, heavy, ceiling, n_random, rng, top_ceiling=None):
+    """Per query: its `heavy` largest counts at or below the ceiling (the
+    first query's largest may reach top_ceiling) and n_random others."""
+    picks = []
+    for k, c in enumerate(counts):
+        idx = np.argsort(-c.astype(np.float64), kind="stable")
+        cap = top_ceiling if (top_ceiling and k == 0) else ceiling
+        chosen = [int(i) for i in idx if 0 < c[i] <= cap][:heavy]
+        rest = np.setdiff1d(np.arange(len(c)), chosen)
+        chosen += [int(i) for i in rng.choice(rest, min(n_random, len(rest)), replace=False)]
+        picks.append(sorted(set(chosen)))
+    return picks
+
+
+def _oracle_check(w, queries, batch, counts, picks):
+    """Oracle counts of the picked updates on the graph state each one sees."""
+    q0 = queries[0]
+    st = orc.Stream(w.nv, w.labels, w.edges, q0.labels, q0.offsets, q0.nbrs)
+    by_update = {}
+    for k, p in enumerate(picks):
+        for i in p:
+            by_update.setdefault(i, []).append(k)
+    prev, compared, heaviest = 0, 0, 0
+    for i in sorted(by_update):
+        st.apply_graph(batch[prev:i])
+        prev = i
+        op, a, b = (int(x) for x in batch[i][:3])
+        for k in by_update[i]:
+            q = queries[k]
+            st.set_query(q.labels, q.offsets, q.nbrs)
+            got = st.probe(op, a, b)
+            assert got == counts[k][i], f"query {k} update {i}: engine {counts[k][i]} oracle {got}"
+            compared += 1
+            heaviest = max(heaviest, int(got))
+    return compared, heaviest
+
+
+def test_c2_full_size_heaviest_updates():
+    w = d.Workload(2, num_batches=1)
+    batch = next(w.batches())
+    counts, signs, st = _engine_counts(w, w.queries, batch)
+    assert counts.sum() > 10 ** 8
+    picks = _pick(counts, heavy=4, ceiling=3 * 10 ** 8, n_random=6, rng=np.random.default_rng(2),
+                  top_ceiling=2 * 10 ** 9)
+    compared, heaviest = _oracle_check(w, w.queries, batch, counts, picks)
+    assert compared >= 3 * 8
+    assert heaviest > 10 ** 8, heaviest
+
+
+def test_c3_full_size_256_queries_one_launch():
+    w = d.Workload(3, num_batches=1)
+    batch = next(w.batches())[:512]
+    counts, signs, st = _engine_counts(w, w.queries, batch)
+    assert counts.shape[0] == 256
+    picks = _pick(counts, heavy=2, ceiling=5 * 10 ** 7, n_random=2, rng=np.random.default_rng(3))
+    compared, heaviest = _oracle_check(w, w.queries, batch, counts, picks)
+    assert compared >= 256 * 2
+
+
+def test_c5_skew_scaled_twelve_vertex_queries():
+    w = d.Workload(5, scale_log2=-4, num_batches=1)
+    deg = np.bincount(w.edges.reshape(-1), minlength=w.nv)
+    assert deg.max() > 10 ** 4  # hub vertices
+    batch = next(w.batches())
+    assert len(batch) == 65536 and (batch[:, 0] == 0).mean() > 0.75
+    counts, signs, st = _engine_counts(w, w.queries, batch)
+    picks = _pick(counts, heavy=2, ceiling=10 ** 8, n_random=2, rng=np.random.default_rng(5))
+    compared, heaviest = _oracle_check(w, w.queries, batch, counts, picks)
+    assert compared >= 64 * 2
+    assert st["donations"] > 0

@@ -192,3 +192,36 @@ def test_cluster_filter_is_sound(seed):
         for u, v in enumerate(f):
             assert (bm[u][v // 32] >> (v % 32)) & 1, f"embedding {f}: vertex {v} pruned for u{u}"
             assert (vc[v] >> u) & 1
+
+
+def test_probe_and_set_query_equal_apply():
+    """probe(update) on the graph before it == the count apply() reports, and
+    one graph serves several queries through set_query."""
+    import dsm_b200 as d  # the seeded workload generator
+    w = d.Workload(3, scale_log2=-8, num_batches=1)
+    ups = next(w.batches())[:200]
+    qs = w.queries[:3]
+    st = orc.Stream(w.nv, w.labels, w.edges, qs[0].labels, qs[0].offsets, qs[0].nbrs)
+    want = []
+    for q in qs:
+        ref = orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs)
+        want.append(ref.apply(ups, listed=False)[1])
+    for i, u in enumerate(ups):
+        for k, q in enumerate(qs):
+            st.set_query(q.labels, q.offsets, q.nbrs)
+            assert st.probe(u[0], u[1], u[2], threads=2) == want[k][i], (i, k)
+        st.apply_graph(ups[i:i + 1])
+
+
+def test_oracle_workload_equals_engine_workload():
+    """The CPU arms generate their inputs through the oracle library; they
+    must be the engine's inputs exactly."""
+    import dsm_b200 as d
+    for cfg, sc in ((1, 0), (3, -8), (4, -12)):
+        a, b = d.Workload(cfg, scale_log2=sc, num_batches=3), orc.Workload(cfg, scale_log2=sc, num_batches=3)
+        assert a.nv == b.nv and np.array_equal(a.labels, b.labels) and np.array_equal(a.edges, b.edges)
+        assert np.array_equal(a.updates, b.updates) and np.array_equal(a.batch_sizes, b.batch_sizes)
+        assert len(a.queries) == len(b.queries)
+        for x, y in zip(a.queries, b.queries):
+            assert np.array_equal(x.labels, y.labels) and np.array_equal(x.offsets, y.offsets)
+            assert np.array_equal(x.nbrs, y.nbrs)
