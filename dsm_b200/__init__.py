@@ -20,7 +20,8 @@ ERR = {1: "PARSE", 2: "OOM", 3: "OVERFLOW", 4: "TIMEOUT", 5: "LIMIT", 6: "ARG", 
 
 OPT_LIST, OPT_FILTER, OPT_RESULT_CAP, OPT_WARPS_PER_SM, OPT_DONATE, OPT_TIMEOUT_MS, OPT_LABEL_QUIRK, OPT_SORT, \
     OPT_LIST_LIMIT, OPT_MEM_BUDGET, OPT_SPLIT_MIN, OPT_DONATE_DEPTH, OPT_AUTOTUNE, OPT_GRAPH, OPT_STALL_TEST, \
-    OPT_PLAIN, OPT_QUERY_LIST_LIMIT = range(1, 18)
+    OPT_PLAIN, OPT_QUERY_LIST_LIMIT, OPT_WORK_LIMIT = range(1, 19)
+INCOMPLETE = np.uint64(1 << 63)  # bit of a count whose search went over DSM_OPT_WORK_LIMIT
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is not built; run `python dsm_b200/build.py`")
@@ -49,7 +50,7 @@ class Stats(C.Structure):
                                           "last_sort_ms")] + [(n, C.c_uint64) for n in (
                    "device_bytes_in_use", "kernel_launches", "query_bytes", "live_queries", "tune_runs")] + \
                [("tune_best_ms", C.c_double)] + [(n, C.c_uint64) for n in (
-                   "graph_launches", "graph_instantiations", "graph_captures", "compactions")]
+                   "graph_launches", "graph_instantiations", "graph_captures", "compactions", "over_limit")]
 
 
 class BatchTiming(C.Structure):
@@ -283,6 +284,14 @@ class BatchResult:
         self.listed = bool(view.listed)
         self.query_listed = _arr(view.query_listed, nq, np.uint8).astype(bool)
         self.num_updates = n
+
+    @property
+    def complete(self):
+        """(queries, updates) mask: the count is exact (not over the work limit)."""
+        return (self.counts & INCOMPLETE) == 0
+
+    def exact_matches(self):
+        return int(self.counts[self.complete].sum())
 
     def query_index(self, qid):
         return int(np.nonzero(self.qids == qid)[0][0])

@@ -98,6 +98,10 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
     case DSM_OPT_GRAPH: E.use_graph = value ? 1 : 0; return DSM_OK;
     case DSM_OPT_STALL_TEST: E.stall_test = value ? 1 : 0; return DSM_OK;
     case DSM_OPT_PLAIN: E.plain = value ? 1 : 0; return DSM_OK;
+    case DSM_OPT_WORK_LIMIT:
+      if (value < 0) return E.fail(DSM_ERR_ARG, "work limit must be >= 0");
+      E.work_limit = (unsigned long long)value;
+      return DSM_OK;
     case DSM_OPT_QUERY_LIST_LIMIT:
       if (value < 0) return E.fail(DSM_ERR_ARG, "per-query listing limit must be >= 0");
       E.query_list_limit = (unsigned long long)value;
@@ -133,6 +137,7 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_GRAPH: *value = E.use_graph; return DSM_OK;
     case DSM_OPT_STALL_TEST: *value = E.stall_test; return DSM_OK;
     case DSM_OPT_PLAIN: *value = E.plain; return DSM_OK;
+    case DSM_OPT_WORK_LIMIT: *value = (int64_t)E.work_limit; return DSM_OK;
     case DSM_OPT_QUERY_LIST_LIMIT: *value = (int64_t)E.query_list_limit; return DSM_OK;
   }
   return E.fail(DSM_ERR_ARG, "unknown option");

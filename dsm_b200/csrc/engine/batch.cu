@@ -154,6 +154,8 @@ int Engine::launch_front(Staged &S) {
       (rc = dalloc(d_dkey, dd * 8)) || (rc = dalloc(d_dhead, (dd + 1) * 4)) || (rc = dalloc(d_dsel, dd * 4)) ||
       (rc = dalloc(d_segcnt, S.nseg * 8)) || (rc = dalloc(d_qlisted, std::max<size_t>(S.nq_live, 1) * 8)))
     return rc;
+  S.work_limit = S.match ? work_limit : 0;
+  if (S.work_limit && (rc = dalloc(d_segwork, S.nseg * 8))) return rc;
   if (S.match && (rc = dalloc(d_seeds, S.seed_cap * 16))) return rc;
   if (!d_jobs.ptr) {
     if ((rc = dalloc(d_jobs, (size_t)job_ring * sizeof(JobRec))) || (rc = dalloc(d_job_seq, (size_t)job_ring * 8)))
@@ -198,8 +200,9 @@ int Engine::launch_front(Staged &S) {
   DevGraph g = dev_graph();
   const BatchHdr *dh = (const BatchHdr *)d_hdr.ptr;
   unsigned int *d_err = (unsigned int *)d_misc.ptr;
-  ClearArgs ca{dh, (uint32_t *)d_vtp.ptr, (unsigned long long *)d_segcnt.ptr, (unsigned long long *)d_qlisted.ptr,
-               (Sched *)d_sched.ptr, (uint32_t *)d_misc.ptr};
+  unsigned long long *segwork = S.work_limit ? (unsigned long long *)d_segwork.ptr : nullptr;
+  ClearArgs ca{dh, (uint32_t *)d_vtp.ptr, (unsigned long long *)d_segcnt.ptr, segwork,
+               (unsigned long long *)d_qlisted.ptr, (Sched *)d_sched.ptr, (uint32_t *)d_misc.ptr};
   EdgeStateArgs es{g, dh, (const uint4 *)d_upd.ptr, (const unsigned long long *)d_bkey.ptr,
                    (const uint32_t *)d_bidx.ptr, (uint32_t *)d_binfo.ptr, (uint8_t *)d_gflag.ptr,
                    (uint32_t *)d_vtp.ptr};
@@ -227,6 +230,8 @@ int Engine::launch_front(Staged &S) {
   ma.seg_count = (unsigned long long *)d_segcnt.ptr;
   ma.qlisted = (unsigned long long *)d_qlisted.ptr;
   ma.qlimit = S.qlimit;
+  ma.work_limit = S.work_limit;
+  ma.seg_work = segwork;
   ma.abort_flag = d_err;
   ma.list = list_mode;
   ma.donate = donate;
@@ -414,6 +419,7 @@ int Engine::finish_device(Staged &S) {
       hs->nseeds = nseeds;
       CK(cudaMemcpyAsync(d_sched.ptr, hs, sizeof(Sched), cudaMemcpyHostToDevice, stream));
       CK(cudaMemsetAsync(d_segcnt.ptr, 0, S.nseg * 8, stream));
+      if (S.work_limit) CK(cudaMemsetAsync(d_segwork.ptr, 0, S.nseg * 8, stream));
       CK(cudaMemsetAsync(d_qlisted.ptr, 0, std::max<size_t>(S.nq_live, 1) * 8, stream));
       launch_sched_init((Sched *)d_sched.ptr, dh, (unsigned long long *)d_job_seq.ptr, job_ring, stream, stall_test);
       ++stats.kernel_launches;
@@ -433,6 +439,8 @@ int Engine::finish_device(Staged &S) {
       ma.seg_count = (unsigned long long *)d_segcnt.ptr;
       ma.qlisted = (unsigned long long *)d_qlisted.ptr;
       ma.qlimit = S.qlimit;
+      ma.work_limit = S.work_limit;
+      ma.seg_work = S.work_limit ? (unsigned long long *)d_segwork.ptr : nullptr;
       ma.abort_flag = (const unsigned int *)d_misc.ptr;
       ma.list = 1;
       ma.donate = donate;
@@ -559,11 +567,19 @@ int Engine::assemble(Staged &S, BatchResult &R) {
   if (S.listed && S.qlimit)
     for (uint32_t ql = 0; ql < nql; ++ql)
       if (S.qlisted[ql] > S.qlimit) R.qlisted[ql] = 0;
+  // a segment over the work limit (bit 63) lists nothing and its count is
+  // partial; the batch's exact matches leave it out
+  uint64_t exact = 0, incomplete = 0;
+  for (uint64_t c : R.counts) {
+    if (c & kCountIncomplete) ++incomplete;
+    else exact += c;
+  }
   R.offsets.assign((size_t)nql * n + 1, 0);
   for (uint32_t ql = 0; ql < nql; ++ql)
     for (uint32_t i = 0; i < n; ++i) {
       const size_t s = (size_t)ql * n + i;
-      R.offsets[s + 1] = R.offsets[s] + (R.qlisted[ql] ? R.counts[s] * R.widths[ql] : 0);
+      const bool lst = R.qlisted[ql] && !(R.counts[s] & kCountIncomplete);
+      R.offsets[s + 1] = R.offsets[s] + (lst ? R.counts[s] * R.widths[ql] : 0);
     }
   R.listed = S.listed;
   R.tuples.clear();
@@ -574,7 +590,7 @@ int Engine::assemble(Staged &S, BatchResult &R) {
     for (size_t r = 0; r < S.cnt; ++r) {
       const uint32_t s = hs[r];
       const uint32_t ql = s / n;
-      if (!R.qlisted[ql]) continue;  // partial tuples of a query past its budget
+      if (!R.qlisted[ql] || (R.counts[s] & kCountIncomplete)) continue;  // partial tuples
       const uint32_t w = R.widths[ql];
       std::memcpy(&R.tuples[cur[s]], ht + r * S.W, w * 4);
       cur[s] += w;
@@ -582,8 +598,10 @@ int Engine::assemble(Staged &S, BatchResult &R) {
     if (S.sort) {
       std::vector<uint64_t> cnt_listed(R.counts);
       for (uint32_t ql = 0; ql < nql; ++ql)
-        if (!R.qlisted[ql])
-          for (uint32_t i = 0; i < n; ++i) cnt_listed[(size_t)ql * n + i] = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+          uint64_t &c = cnt_listed[(size_t)ql * n + i];
+          if (!R.qlisted[ql] || (c & kCountIncomplete)) c = 0;
+        }
       const auto ts = std::chrono::steady_clock::now();
       sort_segments(R, cnt_listed, nql, n, S.cnt);
       R.sort_ms = ms_since(ts);
@@ -593,12 +611,14 @@ int Engine::assemble(Staged &S, BatchResult &R) {
   R.match_ms = S.ms_match;
   R.host_prep_ms = S.host_prep_ms;
   R.alg_bytes = S.sc.alg_bytes;
-  R.matches = S.sc.matches;
+  R.matches = exact;
+  R.incomplete = incomplete;
   {
     std::lock_guard<std::mutex> lk(smu);
     stats.batches++;
     stats.updates += n;
-    stats.matches += S.sc.matches;
+    stats.matches += exact;
+    stats.over_limit += incomplete;
     stats.seeds += S.sc.nseeds;
     stats.donations += S.sc.donations;
     stats.steals += S.sc.steals;
@@ -701,6 +721,7 @@ int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
     hs->nseeds = nseeds;
     CK(cudaMemcpyAsync(d_sched.ptr, hs, sizeof(Sched), cudaMemcpyHostToDevice, stream));
     CK(cudaMemsetAsync(d_segcnt.ptr, 0, S.nseg * 8, stream));
+    if (S.work_limit) CK(cudaMemsetAsync(d_segwork.ptr, 0, S.nseg * 8, stream));
     CK(cudaMemsetAsync(d_qlisted.ptr, 0, std::max<size_t>(S.nq_live, 1) * 8, stream));
     launch_sched_init((Sched *)d_sched.ptr, (const BatchHdr *)d_hdr.ptr, (unsigned long long *)d_job_seq.ptr,
                       job_ring, stream, stall_test);

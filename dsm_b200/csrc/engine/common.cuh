@@ -139,6 +139,10 @@ struct Sched {
   unsigned int pad[5];
 };
 
+// Bit 63 of a (query, update) count: the segment's search went over the
+// work limit; the low bits are a partial count.
+constexpr unsigned long long kCountIncomplete = 1ull << 63;
+
 constexpr unsigned kErrTimeout = 1u;
 constexpr unsigned kErrArena = 2u;
 constexpr unsigned kErrSeeds = 4u;

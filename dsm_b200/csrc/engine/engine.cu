@@ -129,7 +129,7 @@ std::vector<DevBuf *> Engine::all_dev_bufs() {
   std::vector<DevBuf *> v = {&d_lab, &d_adj, &d_cap, &d_arena, &d_arena_top, &d_loff, &d_qd, &d_orders,
                              &d_pair_off, &d_pair_ent, &d_upd, &d_bkey, &d_bidx, &d_binfo, &d_gflag,
                              &d_vtp, &d_dkey, &d_dhead, &d_dsel, &d_seeds, &d_sched, &d_jobs,
-                             &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc, &d_hdr, &d_qlisted};
+                             &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc, &d_hdr, &d_qlisted, &d_segwork};
   for (auto &q : slots) v.push_back(&q.bitmap);
   for (auto &q : slots) v.push_back(&q.filter_scratch);
   for (auto &q : slots) v.push_back(&q.filter_plan);

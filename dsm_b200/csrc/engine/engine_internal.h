@@ -70,7 +70,7 @@ struct Staged {
   size_t nseg = 0;
   unsigned long long seed_cap = 0;
   int plain = 0, sort = 1;
-  unsigned long long qlimit = 0;
+  unsigned long long qlimit = 0, work_limit = 0;
   // after the matcher
   Sched sc{};
   std::vector<unsigned long long> qlisted;
@@ -89,7 +89,7 @@ struct BatchResult {
   std::vector<uint32_t> tuples;
   int listed = 1;
   double device_ms = 0, match_ms = 0, host_prep_ms = 0, sort_ms = 0;
-  uint64_t alg_bytes = 0, matches = 0;
+  uint64_t alg_bytes = 0, matches = 0, incomplete = 0;
   // served timing: submit -> start of the device batch -> results readable
   double queue_ms = 0, service_ms = 0, total_ms = 0;
   uint32_t merged_requests = 1, merged_updates = 0;
@@ -171,6 +171,7 @@ struct Engine {
   int stall_test = 0;                        // arm matcher launches with a task nobody finishes
   int plain = 0;                             // one matcher launch per query (the reference's form)
   unsigned long long query_list_limit = 0;   // tuples one query may list per batch (0: no budget)
+  unsigned long long work_limit = 0;         // partial embeddings per (query, update) (0: no limit)
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   std::string gkey[2];                       // what each executable graph was captured with
   uint64_t seg_kernels[2] = {0, 0};          // kernels each executable graph holds
@@ -198,7 +199,7 @@ struct Engine {
 
   // batch scratch
   DevBuf d_upd, d_bkey, d_bidx, d_binfo, d_gflag, d_vtp, d_dkey, d_dhead, d_dsel, d_seeds, d_sched, d_jobs,
-      d_job_seq, d_out_seg, d_out_tup, d_segcnt, d_misc, d_hdr, d_qlisted;
+      d_job_seq, d_out_seg, d_out_tup, d_segcnt, d_misc, d_hdr, d_qlisted, d_segwork;
   HostBuf h_sched;    // Sched + the error words, read after the matcher
   HostBuf h_qlisted;  // per-query listing counters, read after the matcher
   HostOut hout[2];

@@ -275,6 +275,8 @@ __global__ void k_batch_clear(ClearArgs A) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   for (size_t i = t; i < h.n; i += stride) A.vtp[i] = kNoView;
   for (size_t i = t; i < h.nseg; i += stride) A.segcnt[i] = 0;
+  if (A.segwork)
+    for (size_t i = t; i < h.nseg; i += stride) A.segwork[i] = 0;
   for (size_t i = t; i < h.nq_live; i += stride) A.qlisted[i] = 0;
   uint32_t *sc = reinterpret_cast<uint32_t *>(A.sc);
   for (size_t i = t; i < sizeof(Sched) / 4; i += stride) sc[i] = 0;

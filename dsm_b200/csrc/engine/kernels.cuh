@@ -26,6 +26,7 @@ struct ClearArgs {
   const BatchHdr *hdr;
   uint32_t *vtp;
   unsigned long long *segcnt;
+  unsigned long long *segwork;  // null: no work limit this batch
   unsigned long long *qlisted;
   Sched *sc;
   uint32_t *misc;  // 64 words
@@ -114,6 +115,9 @@ struct MatchArgs {
   // tuples each query asked to list, so the host knows which went over
   unsigned long long *qlisted;
   unsigned long long qlimit;
+  // work limit per (query, update) segment (0 = none): see run_task
+  unsigned long long work_limit;
+  unsigned long long *seg_work;    // [nseg] partial embeddings generated so far
   const unsigned int *abort_flag;  // non-zero (kErrArena): the batch was refused, match nothing
   int list;
   int donate;

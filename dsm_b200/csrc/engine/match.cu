@@ -160,7 +160,26 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
     }
   };
 
+  // Work limit (P.work_limit > 0): `work` counts the valid partial
+  // embeddings of 3 or more positions this task generated (embeddings
+  // included).  The total of a (query, update) segment does not depend on
+  // scheduling, so "the segment's total reached the limit" is deterministic:
+  // whoever's addition crosses it sets bit 63 of the segment's count, and the
+  // segment's tasks stop (its count is then partial, marked by that bit).
+  unsigned long long work = 0;
+  auto publish_work = [&]() -> bool {  // true: the segment is over its limit
+    uint32_t over = 0;
+    if (lane == 0) {
+      const unsigned long long before = work ? atomicAdd(&P.seg_work[seg], work) : ld_volatile(P.seg_work[seg]);
+      over = before + work >= P.work_limit;
+      if (work && before < P.work_limit && over) atomicOr(&P.seg_count[seg], kCountIncomplete);
+    }
+    work = 0;
+    return __shfl_sync(kFull, over, 0) != 0;
+  };
+
   auto flush = [&]() {
+    if (P.work_limit && work) publish_work();
     if (lane == 0) {
       if (task_cnt) {
         atomicAdd(&P.seg_count[seg], task_cnt);
@@ -175,6 +194,7 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
     flush();
     return;
   }
+  if (P.work_limit && publish_work()) return;  // a segment already over its limit
 
   // Level L scans the run of its pivot: the backward neighbour with the
   // fewest candidates (label-major: entries with L's label; plain: degree).
@@ -289,6 +309,7 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
         }
       }
       uint32_t m = __ballot_sync(kFull, ok);
+      work += __popc(m);
       alg += (kLM ? 4ull : 8ull) * min(32u, end - pos) + 4ull * __reduce_add_sync(kFull, probes);
       if (lane == L) {
         lv_pos = pos + 32;
@@ -305,6 +326,7 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
           err = ld_volatile(P.sc->error);
         }
         if (__shfl_sync(kFull, err, 0)) break;
+        if (P.work_limit && publish_work()) break;
       }
       if (P.donate && (ticks & 7) == 0) {
         const uint32_t split_min = P.split_min > 64 ? P.split_min : (P.split_min ? 64u : 128u);

@@ -98,6 +98,17 @@ const char *dsm_last_error(dsm_engine *e);
                                    the default).  A query over it is reported with exact
                                    counts and no tuples for that batch (query_listed = 0 in
                                    the view); the other queries stay listed. */
+#define DSM_OPT_WORK_LIMIT 18   /* bound on the search of one (query, update): the number of
+                                   partial embeddings of 3 or more query vertices it
+                                   generates, embeddings included (0: no bound, the
+                                   default).  That number depends only on the graph, the
+                                   query and the matching order -- not on scheduling -- so
+                                   whether a (query, update) reaches the bound is
+                                   deterministic.  One that does stops early: its count in
+                                   the result view has bit 63 set (low bits: a partial
+                                   count) and it lists no tuples.  Every other count stays
+                                   exact.  (With DSM_OPT_FILTER > 0 the filter prunes
+                                   partial embeddings, so fewer reach the bound.) */
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
 int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
 
@@ -174,7 +185,8 @@ typedef struct dsm_result_view {
   const uint32_t *qids;     /* [num_queries], ascending */
   const uint32_t *widths;   /* [num_queries]: tuple width = query vertex count */
   const int8_t *signs;      /* [num_updates]: +1 insert, -1 delete, 0 no-op update */
-  const uint64_t *counts;   /* [num_queries * num_updates], query-major */
+  const uint64_t *counts;   /* [num_queries * num_updates], query-major; bit 63 set:
+                               the search went over DSM_OPT_WORK_LIMIT (partial count) */
   const uint64_t *offsets;  /* [num_queries * num_updates + 1]: word offsets into tuples */
   const uint32_t *tuples;   /* (f(0)..f(nq-1)) per embedding, each segment sorted */
   int listed;               /* 0 when the batch ran with DSM_OPT_LIST = 0 (or over the
@@ -282,7 +294,7 @@ int dsm_count_edge_embeddings_noalloc(int device, uint32_t nv, const uint32_t *d
 typedef struct dsm_stats {
   uint64_t batches;
   uint64_t updates;
-  uint64_t matches;          /* total |P| + |N| emitted */
+  uint64_t matches;          /* total |P| + |N| emitted (exact counts only) */
   uint64_t seeds;            /* (update, ordered query edge) tasks */
   uint64_t donations;        /* jobs handed from busy to idle warps */
   uint64_t steals;           /* jobs taken from the shared queue */
@@ -304,6 +316,7 @@ typedef struct dsm_stats {
   uint64_t graph_instantiations; /* executable graphs instantiated */
   uint64_t graph_captures;   /* segments captured (a replay reuses the last capture) */
   uint64_t compactions;      /* adjacency arena compactions */
+  uint64_t over_limit;       /* (query, update) searches stopped by DSM_OPT_WORK_LIMIT */
 } dsm_stats;
 int dsm_engine_stats(dsm_engine *e, dsm_stats *s);
 

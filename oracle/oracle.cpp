@@ -619,6 +619,8 @@ int cluster_filter_impl(uint32_t nq, const uint32_t *qlabels, const uint32_t *qo
 // Continuous matching (main.cu:268-329 seeding, gpu_match.cu:947-1118
 // expansion) with per-update sequential semantics.
 // ------------------------------------------------------------------------
+constexpr uint64_t kIncomplete = 1ull << 63;  // count bit: the search reached the work limit
+
 struct Stream {
   uint32_t nv = 0, nq = 0;
   std::vector<uint32_t> labels;
@@ -634,6 +636,7 @@ struct Stream {
   std::vector<uint32_t> tuples;
   uint64_t bytes = 0;
   uint64_t work_budget = ~0ull;  // apply() stops enumerating once `bytes` passes this
+  uint64_t work_limit = 0;       // per-update search bound (struct Work), 0: none
   uint32_t complete = 0;         // updates of the last apply with full results
 
   bool has_edge(uint32_t a, uint32_t b) const {
@@ -642,10 +645,37 @@ struct Stream {
   }
 };
 
+// Search bound per update (the engine's DSM_OPT_WORK_LIMIT): the valid
+// partial embeddings of 3 or more positions the update's search generates,
+// embeddings included, summed over every thread working on the update.  The
+// total depends only on graph, query and order, so "total >= limit" is
+// exact; counts are flushed to the shared total every 256, and a search that
+// sees the total at the limit stops early.
+struct Work {
+  uint64_t limit = 0;  // 0: no bound
+  std::atomic<uint64_t> *total = nullptr;
+  uint64_t local = 0;
+  bool stop = false;
+  bool bump() {  // one more prefix; true: stop searching
+    if (!limit) return false;
+    if (++local < 256) return false;
+    return flush();
+  }
+  bool flush() {
+    if (limit && local) {
+      stop = total->fetch_add(local) + local >= limit;
+      local = 0;
+    } else if (limit) {
+      stop = total->load() >= limit;
+    }
+    return stop;
+  }
+};
+
 void enumerate(const Stream &S, const Stream::Seed &sd, std::vector<uint32_t> &f, size_t p,
-               bool list, uint64_t &cnt, std::vector<uint32_t> &out, uint64_t &bytes) {
+               bool list, uint64_t &cnt, std::vector<uint32_t> &out, uint64_t &bytes, Work &W) {
   const uint32_t nq = S.nq;
-  if (bytes > S.work_budget) return;
+  if (bytes > S.work_budget || W.stop) return;
   if (p == nq) {
     ++cnt;
     if (list) {
@@ -678,20 +708,34 @@ void enumerate(const Stream &S, const Stream::Seed &sd, std::vector<uint32_t> &f
       }
     if (!ok) continue;
     f[p] = w;
-    enumerate(S, sd, f, p + 1, list, cnt, out, bytes);
+    if (W.bump()) return;
+    enumerate(S, sd, f, p + 1, list, cnt, out, bytes, W);
+    if (W.stop) return;
   }
 }
 
+// Embeddings through edge {a, b} of the current graph.  With S.work_limit,
+// a search that reaches the limit returns a partial count with bit 63 set and
+// lists nothing.
 uint64_t match_edge(const Stream &S, uint32_t a, uint32_t b, bool list, std::vector<uint32_t> &out,
                     uint64_t &bytes) {
   uint64_t cnt = 0;
   std::vector<uint32_t> f(S.nq);
   size_t first = out.size();
+  std::atomic<uint64_t> total{0};
+  Work W;
+  W.limit = S.work_limit;
+  W.total = &total;
   for (const auto &sd : S.seeds) {
     if (S.labels[a] != S.qlabels[sd.u] || S.labels[b] != S.qlabels[sd.v]) continue;
     f[0] = a;
     f[1] = b;
-    enumerate(S, sd, f, 2, list, cnt, out, bytes);
+    enumerate(S, sd, f, 2, list, cnt, out, bytes, W);
+    if (W.stop) break;
+  }
+  if (W.limit && W.flush()) {
+    out.resize(first);
+    return cnt | kIncomplete;
   }
   if (list) {
     // canonical order: lexicographic over (f(0), ..., f(nq-1))
@@ -767,7 +811,7 @@ struct Partial {
 };
 
 // Children of a partial embedding (one level of enumerate()).
-void expand_one(const Stream &S, const Partial &x, std::vector<Partial> &out) {
+void expand_one(const Stream &S, const Partial &x, std::vector<Partial> &out, Work &W) {
   const Stream::Seed &sd = S.seeds[x.seed];
   const uint32_t p = x.depth, u = sd.order[p], mask = sd.bn[p];
   int pivot = -1;
@@ -786,6 +830,7 @@ void expand_one(const Stream &S, const Partial &x, std::vector<Partial> &out) {
     y.f[p] = w;
     y.depth = p + 1;
     out.push_back(y);
+    if (W.bump()) return;
   }
 }
 
@@ -805,7 +850,11 @@ uint64_t match_edge_mt(const Stream &S, uint32_t a, uint32_t b, bool list, std::
   // breadth-first until there is enough work to share (or leaves are reached)
   uint64_t done_cnt = 0;
   std::vector<uint32_t> done_tuples;
-  while (!front.empty() && front.size() < (size_t)16 * nt) {
+  std::atomic<uint64_t> total{0};
+  Work W0;
+  W0.limit = S.work_limit;
+  W0.total = &total;
+  while (!front.empty() && front.size() < (size_t)16 * nt && !W0.stop) {
     std::vector<Partial> next;
     for (const Partial &x : front) {
       if (x.depth == S.nq) {
@@ -818,24 +867,32 @@ uint64_t match_edge_mt(const Stream &S, uint32_t a, uint32_t b, bool list, std::
         }
         continue;
       }
-      expand_one(S, x, next);
+      expand_one(S, x, next, W0);
+      if (W0.stop) break;
     }
     front.swap(next);
   }
+  W0.flush();
   std::atomic<size_t> next_task{0};
   std::vector<uint64_t> cnt(nt, 0);
   std::vector<std::vector<uint32_t>> tup(nt);
-  pool.run([&](int t) {
-    std::vector<uint32_t> f(S.nq);
-    uint64_t bytes = 0;
-    for (size_t i; (i = next_task.fetch_add(1)) < front.size();) {
-      const Partial &x = front[i];
-      std::copy(x.f.begin(), x.f.begin() + x.depth, f.begin());
-      enumerate(S, S.seeds[x.seed], f, x.depth, list, cnt[t], tup[t], bytes);
-    }
-  });
-  uint64_t total = done_cnt;
-  for (int t = 0; t < nt; ++t) total += cnt[t];
+  if (!W0.stop)
+    pool.run([&](int t) {
+      std::vector<uint32_t> f(S.nq);
+      uint64_t bytes = 0;
+      Work W;
+      W.limit = S.work_limit;
+      W.total = &total;
+      for (size_t i; (i = next_task.fetch_add(1)) < front.size() && !W.stop;) {
+        const Partial &x = front[i];
+        std::copy(x.f.begin(), x.f.begin() + x.depth, f.begin());
+        enumerate(S, S.seeds[x.seed], f, x.depth, list, cnt[t], tup[t], bytes, W);
+      }
+      W.flush();
+    });
+  uint64_t sum = done_cnt;
+  for (int t = 0; t < nt; ++t) sum += cnt[t];
+  if (S.work_limit && total.load() >= S.work_limit) return sum | kIncomplete;
   if (list) {
     const size_t first = out.size(), w = S.nq;
     out.insert(out.end(), done_tuples.begin(), done_tuples.end());
@@ -853,7 +910,7 @@ uint64_t match_edge_mt(const Stream &S, uint32_t a, uint32_t b, bool list, std::
       std::copy(base + (size_t)idx[i] * w, base + (size_t)idx[i] * w + w, sorted.begin() + i * w);
     std::copy(sorted.begin(), sorted.end(), out.begin() + first);
   }
-  return total;
+  return sum;
 }
 
 void count_all_rec(const Stream &S, const std::vector<uint32_t> &order,
@@ -1155,6 +1212,7 @@ uint64_t orc_stream_probe(orc_stream *h, uint32_t op, uint32_t a, uint32_t b, in
 }
 
 void orc_stream_set_budget(orc_stream *h, uint64_t bytes) { h->s.work_budget = bytes; }
+void orc_stream_set_work_limit(orc_stream *h, uint64_t limit) { h->s.work_limit = limit; }
 uint32_t orc_stream_complete(const orc_stream *h) { return h->s.complete; }
 
 int8_t orc_stream_sign(const orc_stream *s, uint32_t i) { return s->s.sign[i]; }

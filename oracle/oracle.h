@@ -106,6 +106,11 @@ void orc_stream_set_budget(orc_stream *s, uint64_t bytes);
  * results; updates apply in order, each update's search is shared among the
  * threads.  No work budget. */
 int orc_stream_apply_mt(orc_stream *s, uint32_t n, const uint32_t *updates, int list, int threads);
+/* Bound on each update's search (0: none, the default): the valid partial
+ * embeddings of 3 or more query vertices it generates, embeddings included
+ * -- the engine's DSM_OPT_WORK_LIMIT.  An update whose search reaches it
+ * stops; its count then has bit 63 set and it lists nothing. */
+void orc_stream_set_work_limit(orc_stream *s, uint64_t limit);
 /* Replaces the stream's query (the graph stays): one graph, many queries. */
 int orc_stream_set_query(orc_stream *s, uint32_t nq, const uint32_t *qlabels, const uint32_t *qoff,
                          const uint32_t *qnbr);

@@ -45,6 +45,7 @@ _sig("orc_stream_apply", C.c_int, P, C.c_uint32, u32p, C.c_int)
 _sig("orc_stream_apply_mt", C.c_int, P, C.c_uint32, u32p, C.c_int, C.c_int)
 _sig("orc_stream_apply_graph", C.c_int, P, C.c_uint32, u32p)
 _sig("orc_stream_set_query", C.c_int, P, C.c_uint32, u32p, u32p, u32p)
+_sig("orc_stream_set_work_limit", None, P, C.c_uint64)
 _sig("orc_stream_probe", C.c_uint64, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int)
 _sig("orc_stream_set_budget", None, P, C.c_uint64)
 _sig("orc_stream_complete", C.c_uint32, P)
@@ -201,6 +202,10 @@ class Stream:
     def probe(self, op, a, b, threads=-1):
         """Count update (op, a, b) would report now; the graph is unchanged."""
         return lib.orc_stream_probe(self._h, int(op), int(a), int(b), int(threads))
+
+    def set_work_limit(self, limit):
+        """Per-update search bound (the engine's DSM_OPT_WORK_LIMIT)."""
+        lib.orc_stream_set_work_limit(self._h, int(limit))
 
     def set_budget(self, nbytes):
         """Work budget (algorithmic bytes) of each later apply call."""

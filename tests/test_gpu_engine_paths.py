@@ -158,3 +158,43 @@ def test_arena_refusal_leaves_graph_unchanged():
     for x, y in zip(e.export_graph(), st.export()):
         assert np.array_equal(x, y)
     e.close()
+
+
+@pytest.mark.parametrize("form", ["batched", "plain", "graph"])
+def test_work_limit_flags_equal_oracle(form):
+    """DSM_OPT_WORK_LIMIT: the same (query, update) searches go over the
+    bound as in the oracle (whatever the launch form and scheduling), every
+    other count and tuple list is exact, and flagged ones list nothing."""
+    lim = 20_000
+    w = d.Workload(3, scale_log2=-6, num_batches=1)
+    b = next(w.batches())[:512]
+    qs = w.queries[:12]
+    opts = {"OPT_WORK_LIMIT": lim}
+    if form == "plain":
+        opts["OPT_PLAIN"] = 1
+    if form == "graph":
+        opts["OPT_GRAPH"] = 1
+    e, qids = _fresh(w.nv, w.labels, w.edges, qs, **opts)
+    pre = b[:7] if form == "graph" else b[:0]  # graph form: captured on a small batch, replayed
+    b = b[len(pre):]
+    if len(pre):
+        e.run_batch(pre)
+    r = e.run_batch(b)
+    flagged = 0
+    for qid, q in zip(qids, qs):
+        st = oracle_stream(w.nv, w.labels, w.edges, q)
+        st.apply_graph(pre)
+        st.set_work_limit(lim)
+        s, c, t = st.apply(b, listed=True)
+        ql = r.query_index(qid)
+        got = r.counts[ql]
+        fo, fe = (c & d.INCOMPLETE) != 0, (got & d.INCOMPLETE) != 0
+        assert np.array_equal(fo, fe), f"query {qid}: flags differ at {np.nonzero(fo != fe)[0][:10]}"
+        assert np.array_equal(got[~fe], c[~fo])
+        for i in range(len(b)):
+            tt = r.tuples_of(qid, i)
+            assert np.array_equal(tt, t[i] if not fo[i] else t[i][:0]), f"query {qid} update {i}"
+        flagged += int(fe.sum())
+    assert flagged > 0  # the bound was reached somewhere
+    assert e.stats()["over_limit"] >= flagged
+    e.close()

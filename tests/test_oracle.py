@@ -225,3 +225,28 @@ def test_oracle_workload_equals_engine_workload():
         for x, y in zip(a.queries, b.queries):
             assert np.array_equal(x.labels, y.labels) and np.array_equal(x.offsets, y.offsets)
             assert np.array_equal(x.nbrs, y.nbrs)
+
+
+def test_work_limit_flags_do_not_depend_on_threads():
+    """The per-update search bound flags the same updates, with the same
+    exact counts elsewhere, on one thread and on many."""
+    import dsm_b200 as d
+    w = d.Workload(3, scale_log2=-8, num_batches=1)
+    ups = next(w.batches())[:300]
+    INC = np.uint64(1 << 63)
+    for q in w.queries[:6]:
+        a = orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs)
+        full = a.apply(ups, listed=False)[1]
+        a = orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs)
+        b = orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs)
+        lim = int(np.percentile(full[full > 0], 75)) if (full > 0).any() else 10
+        a.set_work_limit(lim)
+        b.set_work_limit(lim)
+        ca = a.apply(ups, listed=False)[1]
+        cb = b.apply(ups, listed=False, threads=4)[1]
+        fa, fb = (ca & INC) != 0, (cb & INC) != 0
+        assert np.array_equal(fa, fb)
+        assert np.array_equal(ca[~fa], cb[~fb])
+        assert np.array_equal(ca[~fa], full[~fa])
+        # an update whose embeddings alone reach the bound is always flagged
+        assert fa[full >= lim].all()
