@@ -9,6 +9,7 @@
 // 2e + 1) and `keep` is allocated as main.cu:76-77 does.
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 #include "cpuGraph.h"
 #include "decycle.h"
@@ -106,5 +107,73 @@ int ref_order(uint32_t nq, uint32_t ne, const uint32_t *edges, uint32_t u, uint3
   }
   return 0;
 }
+
+// ---- data graph and updateHostGraph (cpuGraph.cpp:521-607) ---------------
+// A data cpuGraph filled as readGraphToCPUDynamic fills it (io.cu:122-252):
+// CSR over both directions, each list in file order of the edges.
+void *ref_graph_new(uint32_t nv, const uint32_t *labels, uint64_t ne, const uint32_t *edges) {
+  auto *g = new cpuGraph();
+  g->isQuery = false;
+  g->num_v = nv;
+  g->num_e = (numtype)ne;
+  g->vertexIDs_ = new vtype[nv];
+  g->offsets_ = new offtype[nv + 1];
+  g->outdeg_ = new degtype[nv];
+  g->vLabels_ = new vltype[nv];
+  g->neighbors_ = new vtype[2 * ne + 1];
+  std::memset(g->outdeg_, 0, sizeof(degtype) * nv);
+  for (uint64_t e = 0; e < ne; ++e) {
+    g->outdeg_[edges[2 * e]]++;
+    g->outdeg_[edges[2 * e + 1]]++;
+  }
+  g->offsets_[0] = 0;
+  for (uint32_t v = 0; v < nv; ++v) {
+    g->vertexIDs_[v] = v;
+    g->vLabels_[v] = labels[v];
+    g->offsets_[v + 1] = g->offsets_[v] + g->outdeg_[v];
+  }
+  uint32_t *fill = new uint32_t[nv]();
+  for (uint64_t e = 0; e < ne; ++e) {
+    const uint32_t a = edges[2 * e], b = edges[2 * e + 1];
+    g->neighbors_[g->offsets_[a] + fill[a]++] = b;
+    g->neighbors_[g->offsets_[b] + fill[b]++] = a;
+  }
+  delete[] fill;
+  return g;
+}
+
+// One batch through the reference's updateHostGraph; updates are 4 words
+// each (op 1 = add, src, dst, label).  The reference replaces neighbors_
+// without freeing the old array; the harness frees it afterwards.
+int ref_graph_update(void *h, uint32_t n, const uint32_t *ups) {
+  cpuGraph &g = *static_cast<cpuGraph *>(h);
+  std::vector<change> batch(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    batch[i].add = ups[4 * i] == 1;
+    batch[i].src = ups[4 * i + 1];
+    batch[i].dst = ups[4 * i + 2];
+    batch[i].labelChange = ups[4 * i + 3];
+  }
+  vtype *old = g.neighbors_;
+  updateHostGraph(g, batch);
+  if (old != g.neighbors_) delete[] old;
+  return 0;
+}
+
+// The graph as a CSR (off: nv + 1 words; nbr may be null to size it) and
+// the labels.  Returns the number of neighbour entries.
+uint64_t ref_graph_export(void *h, uint32_t *off, uint32_t *nbr, uint32_t *labels) {
+  const cpuGraph &g = *static_cast<cpuGraph *>(h);
+  const uint64_t total = g.offsets_[g.num_v];
+  if (off)
+    for (uint32_t v = 0; v <= g.num_v; ++v) off[v] = g.offsets_[v];
+  if (nbr)
+    for (uint64_t k = 0; k < total; ++k) nbr[k] = g.neighbors_[k];
+  if (labels)
+    for (uint32_t v = 0; v < g.num_v; ++v) labels[v] = g.vLabels_[v];
+  return total;
+}
+
+void ref_graph_free(void *h) { delete static_cast<cpuGraph *>(h); }
 
 }  // extern "C"

@@ -104,3 +104,67 @@ def test_decycle_and_order_against_reference(k, ascending):
                 assert np.array_equal(ob, rb), (u, v)
             else:
                 assert np.array_equal(ob & rb, rb), (u, v)  # the reference's masks miss some
+
+
+def _ref_graph_lib():
+    lib = C.CDLL(LIB)
+    u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+    lib.ref_graph_new.restype = C.c_void_p
+    lib.ref_graph_new.argtypes = [C.c_uint32, u32p, C.c_uint64, u32p]
+    lib.ref_graph_update.argtypes = [C.c_void_p, C.c_uint32, u32p]
+    lib.ref_graph_export.restype = C.c_uint64
+    lib.ref_graph_export.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ref_graph_free.argtypes = [C.c_void_p]
+    return lib
+
+
+def _ref_export(lib, h, nv):
+    off = np.zeros(nv + 1, np.uint32)
+    n = lib.ref_graph_export(h, off.ctypes.data, None, None)
+    nb = np.zeros(max(n, 1), np.uint32)
+    lib.ref_graph_export(h, off.ctypes.data, nb.ctypes.data, None)
+    return off, nb[:n]
+
+
+def test_update_host_graph_pins_batch_application():
+    """The oracle's batch application (set semantics, updates in stream order)
+    against the reference's updateHostGraph (cpuGraph.cpp:521-607), run on
+    the same data graph batch after batch.  The reference applies a batch
+    sorted by (src, dst) rather than in stream order, so the two agree on
+    every batch that names each edge once: the generated batches, each edge
+    kept at its first occurrence, are checked here; a batch that inserts and
+    deletes one edge is order-dependent in the reference (recorded below)."""
+    import dsm_b200 as d
+    lib = _ref_graph_lib()
+    w = d.Workload(2, scale_log2=-8, num_batches=6)
+    q = w.queries[0]
+    h = lib.ref_graph_new(w.nv, w.labels, len(w.edges), np.ascontiguousarray(w.edges.reshape(-1)))
+    st = orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs)
+    try:
+        for k, b in enumerate(w.batches()):
+            keys = np.minimum(b[:, 1], b[:, 2]).astype(np.uint64) << 32 | np.maximum(b[:, 1], b[:, 2])
+            _, first = np.unique(keys, return_index=True)
+            b = np.ascontiguousarray(b[np.sort(first)])
+            assert len(b) > 3000
+            lib.ref_graph_update(h, len(b), np.ascontiguousarray(b.reshape(-1)))
+            st.apply_graph(b)
+            roff, rnb = _ref_export(lib, h, w.nv)
+            ooff, onb = st.export()
+            assert np.array_equal(roff, ooff) and np.array_equal(rnb, onb), f"batch {k}"
+        # the recorded difference: insert then delete of one absent edge in
+        # one batch -- in stream order the edge ends absent; the reference
+        # sorts the two changes by (src, dst) only, so its outcome depends on
+        # the sort's order of equal keys
+        a, b_ = 0, 1
+        while st.export()[1][st.export()[0][a]:st.export()[0][a + 1]].tolist().count(b_):
+            b_ += 1
+        pair = np.array([[1, a, b_, w.labels[a]], [0, a, b_, w.labels[a]]], np.uint32)
+        st.apply_graph(pair)
+        lib.ref_graph_update(h, 2, np.ascontiguousarray(pair.reshape(-1)))
+        roff, rnb = _ref_export(lib, h, w.nv)
+        ooff, onb = st.export()
+        ref_has = b_ in rnb[roff[a]:roff[a + 1]].tolist()
+        assert b_ not in onb[ooff[a]:ooff[a + 1]].tolist()
+        print(f"insert+delete of one edge in a batch: reference keeps the edge: {ref_has}")
+    finally:
+        lib.ref_graph_free(h)
