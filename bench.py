@@ -1,29 +1,51 @@
 #!/usr/bin/env python
-"""Benchmark: continuous subgraph matching on one B200 (config 2).
+"""Benchmark: continuous subgraph matching on one B200.
 
-Workload (seeded, synthetic; the reference's dataset is not available):
-Chung-Lu power-law graph (exponent 2.1), 2^20 vertices, 2^24 undirected
-edges (10% withheld for re-insertion), 16 Zipf(1.2) labels; three 8-vertex
-random-walk queries (tree, one cycle, 14 edges); batches of 4096 updates,
-50% inserts from the withheld pool, 50% deletes of live edges.
+Default workload (--config 4, the serving loop at full size; seeded and
+synthetic, the reference's dataset is not available): R-MAT(0.57, 0.19,
+0.19) with 2^24 vertices and 2^28 undirected edges (10 % withheld for
+re-insertion), 32 uniform vertex labels; update requests of lognormal size
+(median 512, capped at 65,536 updates), 60 % inserts / 40 % deletes; a pool
+of 64 random-walk queries of 4-10 vertices, all registered at the start, and
+query churn: every 4th request arrives with a registration (a pool query) or
+a retirement (an initial query), alternately.
 
-A step is one update batch matched against the three queries, exact counts
-per update (--list 1 lists and sorts the embeddings as well).  Forms:
-  batched (default): one engine, all queries in one persistent launch;
-  plain: one engine per query, one launch per query (the reference's
-         one-query-per-process form).
-The first warm-up batch autotunes the matcher's launch setting (--autotune).
+The same requests, arrival times and churn run through three forms of the
+engine, each from the same initial graph (between forms the graph is put
+back by applying the inverse of every effective update, without matching):
+  served:  the serving loop -- continuous batching of queued requests into one
+           device batch, host assembly of batch k overlapping device batch
+           k + 1, each device batch replayed from captured CUDA graphs;
+  batched: one request at a time, every registered query in one persistent
+           matcher launch (DSM_OPT_PLAIN = 0), no overlap;
+  plain:   one request at a time, one matcher launch per query with a host
+           round trip after each -- the reference's one-query-per-process loop.
+Every form lists the per-update positive / negative embeddings (canonically
+sorted).  Each (query, update) search is bounded by DSM_OPT_WORK_LIMIT
+(partial embeddings generated): a pair over it is flagged identically in
+every form (and in the oracle); all other counts are exact, and the forms'
+exact match totals and flags must agree request by request.
 
-Prints one JSON line.  `value` = delta-matches per second of device time
-(CUDA events around each batch's device work); `e2e` = the same through the
-C ABI with host buffers (host prep, H2D, matching, D2H, result assembly) on
-the wall clock; `cpu_baseline` = the oracle's all-cores matcher on a prefix
-of the first timed batch (counts).  --impl reference: the CPU arm (the same
-oracle port, all host threads, a bounded prefix of each timed batch).
---mode serve: served vs batched vs plain on the config-4 request stream
-(throughput under a burst, p50 / p99 latency under Poisson arrivals).
+Phases: W * 16 warm-up requests (untimed; the first tunes the matcher's
+launch shape), then K * 16 requests at once (burst: throughput), then K * 16
+requests arriving as a Poisson process at 70 % of the batched form's burst
+request rate (latency from arrival to sorted results readable on the host).
+A step is 16 requests.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode step|serve]
+Prints one JSON line.  `value` = the served form's exact delta-matches per
+second of device time over the burst (events around each device batch;
+inputs copied from host memory inside it); `e2e` = the same matches over the
+burst's wall time through the C ABI (host buffers in, sorted tuples out);
+`latency_ms` = served p50 / p99 in the Poisson phase; `forms` = all three.
+`cpu_baseline` = the oracle's all-cores matcher on a uniform sample of the
+burst's updates (each update on the graph state it sees, every live query).
+--impl reference: the CPU arm -- the same oracle port on that sample (the
+reference has no CPU matcher and its GPU matcher is unwired), plus the
+reference's own updateHostGraph timed on request batches.
+--mode step: config 2 (2^20 vertices, 2^24 edges, three 8-vertex queries,
+batches of 4096), one batch per step, counts only.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode serve|step]
 """
 import argparse
 import json
@@ -37,6 +59,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+
+REQ_PER_STEP = 16
+INCOMPLETE = np.uint64(1 << 63)
 
 
 def _peaks():
@@ -111,428 +136,520 @@ def combine_over_ranks(dev_ms, wall_ms, matches, device):
     return float(mx[0]), float(mx[1]), int(sm[2])
 
 
-def make_workload(steps, warmup, scale):
+def summarize(lat_ms, matches, updates, span_s):
+    lat = np.sort(np.asarray(lat_ms, dtype=np.float64))
+    return {"p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+            "matches_per_sec": matches / span_s if span_s > 0 else 0.0,
+            "updates_per_sec": updates / span_s if span_s > 0 else 0.0, "span_s": span_s,
+            "matches": int(matches)}
+
+
+# ---------------------------------------------------------------------------
+# the serving comparison (config 4)
+# ---------------------------------------------------------------------------
+def churn_schedule(n_req, n_initial, n_pool, every=4, seed=4):
+    """events[k]: the control requests that arrive with request k, in order:
+    ("reg", pool index) or ("ret", index of an initial query).  Alternates
+    registration and retirement; each initial query retires at most once, so
+    every form can name it by the id it got at the start."""
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(n_initial)
+    events, j, r = [[] for _ in range(n_req)], 0, 0
+    for k in range(every - 1, n_req, every):
+        if j % 2 == 0:
+            events[k].append(("reg", int(rng.integers(n_pool))))
+        elif r < n_initial - 1:
+            events[k].append(("ret", int(order[r])))
+            r += 1
+        j += 1
+    return events
+
+
+def exact_matches(counts):
+    c = np.asarray(counts, dtype=np.uint64)
+    ok = (c & INCOMPLETE) == 0
+    return int(c[ok].sum()), int((~ok).sum())
+
+
+class FormRun:
+    """Per-request outcomes of one form."""
+
+    def __init__(self, n):
+        self.matches = np.zeros(n, np.int64)
+        self.flagged = np.zeros(n, np.int64)
+        self.lat = np.zeros(n)
+        self.dev_ms = np.zeros(n)  # this request's share of its device batch
+        self.signs = [None] * n
+        self.merged = np.ones(n)
+        self.d2h = np.zeros(n, np.int64)
+
+    def record(self, k, r, t):
+        m, f = exact_matches(r.counts)
+        self.matches[k], self.flagged[k] = m, f
+        self.signs[k] = r.signs
+        self.lat[k] = t["total_ms"]
+        self.merged[k] = t["merged_requests"]
+        self.dev_ms[k] = t["device_ms"] / max(t["merged_requests"], 1)
+        self.d2h[k] = r.tuples.nbytes + r.counts.nbytes + r.signs.nbytes
+
+
+def run_sync(e, reqs, arrivals, events, pool, initial_ids, base_k, out):
+    """One request at a time in arrival order (batched and plain forms);
+    control requests are applied before the request they arrive with."""
+    t0 = time.perf_counter()
+    for j, b in enumerate(reqs):
+        k = base_k + j
+        now = time.perf_counter() - t0
+        if now < arrivals[j]:
+            time.sleep(arrivals[j] - now)
+        for kind, x in events[k]:
+            if kind == "reg":
+                e.register(pool[x])
+            else:
+                e.retire(initial_ids[x])
+        bid = e.submit(b)
+        t = e.timing(bid)
+        r = e.results(bid)
+        t = dict(t)
+        t["total_ms"] = (time.perf_counter() - t0 - arrivals[j]) * 1e3
+        out.record(k, r, t)
+    return time.perf_counter() - t0
+
+
+def run_served(e, reqs, arrivals, events, pool, initial_ids, base_k, out):
+    """Requests (and control requests) submitted on their arrival times from
+    a submitter thread; results read in order as they become final."""
+    bids = [None] * len(reqs)
+    err = []
+    t0 = time.perf_counter()
+
+    def submitter():
+        try:
+            for j, b in enumerate(reqs):
+                now = time.perf_counter() - t0
+                if now < arrivals[j]:
+                    time.sleep(arrivals[j] - now)
+                for kind, x in events[base_k + j]:
+                    if kind == "reg":
+                        e.register_async(pool[x])
+                    else:
+                        e.retire_async(initial_ids[x])
+                bids[j] = e.submit(b)
+        except Exception as ex:  # surfaced after the reader is done
+            err.append(ex)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    for j in range(len(reqs)):
+        while bids[j] is None:
+            if err:
+                raise err[0]
+            time.sleep(0.0002)
+        t = e.timing(bids[j])
+        r = e.results(bids[j])
+        out.record(base_k + j, r, t)
+    th.join()
+    if err:
+        raise err[0]
+    return time.perf_counter() - t0
+
+
+def restore(e, reqs, runs_signs, initial):
+    """Puts the initial graph and query set back: the inverse of every
+    effective update, newest first, applied without matching; then every
+    query retired and the initial ones registered again (same ids)."""
+    inv = []
+    for b, s in zip(reversed(reqs), reversed(runs_signs)):
+        eff = np.nonzero(s)[0][::-1]
+        if len(eff):
+            u = b[eff].copy()
+            u[:, 0] = 1 - u[:, 0]
+            inv.append(u)
+    if inv:
+        allinv = np.concatenate(inv)
+        for i in range(0, len(allinv), 1 << 20):
+            e.apply_graph(allinv[i:i + (1 << 20)])
+    for qid in e.live_queries():
+        e.retire(qid)
+    ids = [e.register(q) for q in initial]
+    return ids
+
+
+def run_serve(args, rank=0, world=1):
+    import torch
+
     import dsm_b200 as d
-    nb = steps + warmup
-    return d.Workload(2, scale_log2=scale, num_batches=nb)
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    W, K = args.warmup * REQ_PER_STEP, args.steps * REQ_PER_STEP
+    n_req = W + 2 * K
+    t0 = time.time()
+    w = d.Workload(4, scale_log2=args.scale, num_batches=n_req)
+    gen_s = time.time() - t0
+    reqs = list(w.batches())[:n_req]
+    pool = w.queries
+    initial = pool[:args.queries]
+    events = churn_schedule(n_req, len(initial), len(pool))
+    print(f"[bench] config 4: {w.nv} vertices, {len(w.edges)} edges, {len(pool)} pool queries "
+          f"({min(q.nv for q in pool)}-{max(q.nv for q in pool)} vertices), {n_req} requests "
+          f"(median {int(np.median([len(r) for r in reqs]))} updates), generated in {gen_s:.0f} s",
+          file=sys.stderr, flush=True)
+    e = d.Engine(dev)
+    e.set_option(d.OPT_LIST, 1)
+    e.set_option(d.OPT_WORK_LIMIT, args.work_limit)
+    e.set_option(d.OPT_QUERY_LIST_LIMIT, args.query_list_limit)
+    t0 = time.time()
+    e.load_graph_edges(w.nv, w.labels, w.edges)
+    load_s = time.time() - t0
+    ids = [e.register(q) for q in initial]
+    print(f"[bench] graph loaded in {load_s:.0f} s; {e.stats()['device_bytes_in_use'] / 2**30:.1f} GiB on the device",
+          file=sys.stderr, flush=True)
+
+    runs, spans, stats = {}, {}, {}
+    arrivals_burst = np.zeros(K)
+    order = ["batched", "served", "plain"]
+    rate = None
+    sampler = ClockSampler(dev)
+    for fi, form in enumerate(order):
+        run = FormRun(n_req)
+        e.set_option(d.OPT_PLAIN, int(form == "plain"))
+        e.set_option(d.OPT_GRAPH, int(form == "served"))
+        if fi == 0 and args.autotune:
+            e.set_option(d.OPT_AUTOTUNE, 1)
+        s0 = e.stats()
+        if form == "served":
+            e.serve_start(args.serve_merge)
+            runner = run_served
+        else:
+            runner = run_sync
+        runner(e, reqs[:W], np.zeros(W), events, pool, ids, 0, run)
+        torch.cuda.synchronize()
+        s1 = e.stats()
+        if fi == 0:
+            sampler.start()
+        torch.cuda.synchronize()
+        span_b = runner(e, reqs[W:W + K], arrivals_burst, events, pool, ids, W, run)
+        torch.cuda.synchronize()
+        s2 = e.stats()
+        if rate is None:
+            rate = args.load * K / span_b
+            rng = np.random.default_rng(4)
+            arrivals_p = np.cumsum(rng.exponential(1.0 / rate, K))
+        span_p = runner(e, reqs[W + K:], arrivals_p, events, pool, ids, W + K, run)
+        torch.cuda.synchronize()
+        s3 = e.stats()
+        if form == "served":
+            e.serve_stop()
+        spans[form] = (span_b, span_p)
+        stats[form] = (s1, s2, s3)
+        runs[form] = run
+        print(f"[bench] {form}: burst {span_b:.2f} s, poisson {span_p:.2f} s, "
+              f"exact matches {int(run.matches[W:].sum())}, flagged {int(run.flagged[W:].sum())}",
+              file=sys.stderr, flush=True)
+        if fi < len(order) - 1:
+            again = restore(e, reqs, run.signs, initial)
+            assert again == ids, "the initial queries came back with other ids"
+    clocks = sampler.stop()
+
+    # the forms must agree request by request
+    ref = runs["batched"]
+    for form in order[1:]:
+        assert np.array_equal(runs[form].matches, ref.matches), f"{form}: exact matches differ from batched"
+        assert np.array_equal(runs[form].flagged, ref.flagged), f"{form}: over-limit flags differ from batched"
+
+    def form_summary(form):
+        run, (span_b, span_p) = runs[form], spans[form]
+        s1, s2, s3 = stats[form]
+        mb = int(run.matches[W:W + K].sum())
+        ub = int(sum(len(r) for r in reqs[W:W + K]))
+        dev_ms = float(run.dev_ms[W:W + K].sum())
+        burst = summarize(run.lat[W:W + K], mb, ub, span_b)
+        pois = summarize(run.lat[W + K:], int(run.matches[W + K:].sum()), int(sum(len(r) for r in reqs[W + K:])),
+                         span_p)
+        return {"burst": burst, "poisson": pois,
+                "device_matches_per_sec": mb / (dev_ms / 1e3) if dev_ms > 0 else 0.0,
+                "device_updates_per_sec": ub / (dev_ms / 1e3) if dev_ms > 0 else 0.0,
+                "device_ms_burst": dev_ms,
+                "flagged_pairs": int(run.flagged[W:].sum()),
+                "kernel_launches_burst": int(s2["kernel_launches"] - s1["kernel_launches"]),
+                "mean_requests_per_device_batch": float(np.mean(run.merged[W:W + K])),
+                "donations": int(s2["donations"] - s1["donations"]), "steals": int(s2["steals"] - s1["steals"]),
+                "alg_bytes_burst": int(s2["alg_bytes"] - s1["alg_bytes"]),
+                "graph_instantiations": int(s3["graph_instantiations"] - s1["graph_instantiations"]),
+                "graph_captures": int(s3["graph_captures"] - s1["graph_captures"]),
+                "compactions": int(s3["compactions"])}
+
+    forms = {f: form_summary(f) for f in order}
+    sv = forms["served"]
+    mb = sv["burst"]["matches"]
+    h2d = int(sum(r.nbytes for r in reqs[W:W + K]) / args.steps)
+    d2h = int(runs["served"].d2h[W:W + K].sum() / args.steps)
+    peak, peak_kind = _peaks()
+    s1, s2, _ = stats["served"]
+    match_ms = float(runs["served"].dev_ms[W:W + K].sum())
+    alg = sv["alg_bytes_burst"]
+    line = {
+        "metric": "served_delta_matches_per_sec",
+        "value": sv["device_matches_per_sec"],
+        "unit": "matches/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": sv["device_ms_burst"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded R-MAT graph, random-walk queries, generated request stream)",
+        "config": {"workload": f"config4: R-MAT(0.57,0.19,0.19) |V|=2^{24 + args.scale}, |E|=2^{28 + args.scale}, "
+                               f"32 uniform labels, {len(initial)} initial queries of a 64-query pool (4-10 "
+                               f"vertices), churn every 4th request, lognormal requests (median 512, cap 65536), "
+                               f"60% inserts",
+                   "step": f"{REQ_PER_STEP} requests", "listing": True, "work_limit": args.work_limit,
+                   "query_list_limit": args.query_list_limit, "poisson_load": args.load,
+                   "poisson_rate_per_s": rate, "parallelism": f"replicas x{world}",
+                   "l2": "inputs (2^28-edge graph, ~5 GB of runs) far larger than L2"},
+        "updates_per_sec": sv["device_updates_per_sec"],
+        "latency_ms": {"p50": sv["poisson"]["p50_ms"], "p99": sv["poisson"]["p99_ms"]},
+        "matches": mb,
+        "e2e": {"value": sv["burst"]["matches_per_sec"], "unit": "matches/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "updates_per_sec": sv["burst"]["updates_per_sec"]},
+        "forms": forms,
+        "served_vs_plain": {
+            "burst_matches_per_sec": sv["burst"]["matches_per_sec"] / max(forms["plain"]["burst"]["matches_per_sec"],
+                                                                          1e-9),
+            "p99_ratio": (forms["plain"]["poisson"]["p99_ms"] or 0) / max(sv["poisson"]["p99_ms"] or 1e-9, 1e-9)},
+        "gpu_launches": sv["kernel_launches_burst"],
+        "roofline": {"bound": "hbm", "kernel": "k_match", "achieved": alg / 1e9 / (match_ms / 1e3) if match_ms else 0,
+                     "peak": peak, "unit": "GB/s", "peak_source": peak_kind, "traffic": None,
+                     "note": "algorithmic bytes of the matcher over the served device time of the burst"},
+        "clocks": clocks,
+        "gen_seconds": gen_s,
+        "load_seconds": load_s,
+    }
+    line["roofline"]["frac"] = line["roofline"]["achieved"] / peak
+    e.close()
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(w, reqs, W, K, initial, pool, events, args.cpu_s, args.work_limit)
+    return line
 
 
-def run_ours(args, rank, world):
+# ---------------------------------------------------------------------------
+# CPU: the oracle port on a uniform sample
+# ---------------------------------------------------------------------------
+def cpu_sample(w, reqs, W, K, initial, pool, events, budget_s, work_limit, threads=None):
+    """The oracle's all-cores matcher on updates sampled uniformly (fixed
+    seed) from the burst's requests, each counted for every live query on the
+    graph state it sees, until about budget_s seconds of matching; the rest
+    of the stream only moves the oracle's graph."""
+    from oracle import oracle as orc
+    threads = threads or (os.cpu_count() or 1)
+    q0 = initial[0]
+    st = orc.Stream(w.nv, w.labels, w.edges, q0.labels, q0.offsets, q0.nbrs)
+    st.set_work_limit(work_limit)
+    live = list(range(len(initial)))  # pool indices of live queries (initial = pool[:n])
+    init_live = {i: i for i in range(len(initial))}
+    rng = np.random.default_rng(7)
+    n_burst = sum(len(r) for r in reqs[W:W + K])
+    per_update = max(1, n_burst // 256)
+    secs, matches, probes, sampled = 0.0, 0, 0, 0
+    for k, b in enumerate(reqs[:W + K]):
+        for kind, x in events[k]:
+            if kind == "reg":
+                live.append(x)
+            else:
+                live.remove(init_live[x])
+        if k < W or secs >= budget_s:
+            st.apply_graph(b)
+            continue
+        pick = np.nonzero(rng.random(len(b)) < 1.0 / per_update)[0]
+        prev = 0
+        for i in pick:
+            st.apply_graph(b[prev:i])
+            prev = int(i)
+            op, a, c = (int(v) for v in b[i][:3])
+            for qi in live:
+                q = pool[qi]
+                st.set_query(q.labels, q.offsets, q.nbrs)
+                t = time.perf_counter()
+                cnt = st.probe(op, a, c, threads)
+                secs += time.perf_counter() - t
+                probes += 1
+                if not (cnt >> 63):
+                    matches += cnt
+            sampled += 1
+        st.apply_graph(b[prev:])
+    return {"value": matches / secs if secs > 0 else 0.0, "unit": "matches/s", "cores": threads, "kind": "port",
+            "sample": f"{sampled} updates sampled uniformly from the burst's requests (1 in {per_update}), each "
+                      f"counted for every live query ({probes} counts) on the graph state it sees, "
+                      f"{threads} threads, work limit {work_limit}", "seconds": secs}
+
+
+def reference_update_host_graph(w, reqs, n_calls, budget_s):
+    """The reference's own updateHostGraph (cpuGraph.cpp:521-607, compiled
+    from its sources into oracle/_ref/libref.so) on request batches of the
+    same stream: updates per second of its host path.  None when the library
+    was not built."""
+    import ctypes as C
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libref.so")
+    if not os.path.exists(lib_path):
+        return None
+    lib = C.CDLL(lib_path)
+    u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+    lib.ref_graph_new.restype = C.c_void_p
+    lib.ref_graph_new.argtypes = [C.c_uint32, u32p, C.c_uint64, u32p]
+    lib.ref_graph_update.argtypes = [C.c_void_p, C.c_uint32, u32p]
+    lib.ref_graph_free.argtypes = [C.c_void_p]
+    h = lib.ref_graph_new(w.nv, w.labels, len(w.edges), np.ascontiguousarray(w.edges.reshape(-1)))
+    secs, ups, calls = 0.0, 0, 0
+    try:
+        for b in reqs[:n_calls]:
+            t = time.perf_counter()
+            lib.ref_graph_update(h, len(b), np.ascontiguousarray(b.reshape(-1)))
+            secs += time.perf_counter() - t
+            ups += len(b)
+            calls += 1
+            if secs > budget_s:
+                break
+    finally:
+        lib.ref_graph_free(h)
+    return {"updates_per_sec": ups / secs if secs > 0 else 0.0, "calls": calls, "updates": ups, "seconds": secs,
+            "cores": 1, "kind": "reference",
+            "sample": f"the first {calls} requests, one updateHostGraph call each (rebuilds the whole CSR)"}
+
+
+def run_reference(args, rank):
+    """The CPU arm of the serving comparison: the oracle port on a uniform
+    sample of the same burst (each step: the sample's share), plus the
+    reference's own updateHostGraph on the same requests.  The inputs come
+    from the engine's generator compiled into the oracle library; the engine
+    library is not loaded."""
+    if rank != 0:
+        return None
+    from oracle import oracle as orc
+    W, K = args.warmup * REQ_PER_STEP, args.steps * REQ_PER_STEP
+    w = orc.Workload(4, scale_log2=args.scale, num_batches=W + 2 * K)
+    reqs = list(w.batches())[:W + 2 * K]
+    initial = w.queries[:args.queries]
+    events = churn_schedule(W + 2 * K, len(initial), len(w.queries))
+    cb = cpu_sample(w, reqs, W, K, initial, w.queries, events, args.ref_s, args.work_limit)
+    v = cb["value"]
+    line = {"impl": "reference", "metric": "served_delta_matches_per_sec", "value": v, "unit": "matches/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cb["seconds"] / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (the GPU arm's seeded inputs)",
+            "config": {"workload": "config4 (as the GPU arm)", "form": "CPU, per update, all host threads"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_ref_host:
+        line["reference_update_host_graph"] = reference_update_host_graph(w, reqs[W:], 3, args.ref_host_s)
+    return line
+
+
+# ---------------------------------------------------------------------------
+# --mode step: config 2, one 4096-update batch per step (counts)
+# ---------------------------------------------------------------------------
+def run_step(args, rank, world):
     import torch
 
     import dsm_b200 as d
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     t0 = time.time()
-    w = make_workload(args.steps, args.warmup, args.scale)
+    w = d.Workload(2, scale_log2=args.scale, num_batches=args.steps + args.warmup)
     gen_s = time.time() - t0
     batches = list(w.batches())
-    queries = w.queries
-    print(f"[bench] workload generated in {gen_s:.1f} s: {w.nv} vertices, {len(w.edges)} edges, "
-          f"queries {[q.labels.tolist() for q in queries]}", file=sys.stderr, flush=True)
-
-    def new_engine(qs):
-        e = d.Engine(dev)
-        e.set_option(d.OPT_LIST, args.list)
-        e.set_option(d.OPT_FILTER, args.filter)
-        if args.autotune and args.warmup > 0:  # the first warm-up batch picks the launch setting
-            e.set_option(d.OPT_AUTOTUNE, 1)
-        e.load_graph_edges(w.nv, w.labels, w.edges)
-        return e, [e.register(q) for q in qs]
-
-    if args.form == "batched":
-        engines = [new_engine(queries)]
-    else:
-        engines = [new_engine([q]) for q in queries]
-    print(f"[bench] {len(engines)} engine(s) loaded", file=sys.stderr, flush=True)
+    e = d.Engine(dev)
+    e.set_option(d.OPT_LIST, 0)
+    if args.autotune and args.warmup > 0:
+        e.set_option(d.OPT_AUTOTUNE, 1)
+    e.load_graph_edges(w.nv, w.labels, w.edges)
+    for q in w.queries:
+        e.register(q)
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MiB > L2
-
-    def step(b):
-        """One batch through every engine; device ms, wall ms, matches, stats deltas."""
-        dev_ms = wall_ms = match_ms = 0.0
-        matches = alg = launches = 0
-        h2d = d2h = 0
-        for e, qids in engines:
-            s0 = e.stats()
-            torch.cuda.synchronize()
-            tw = time.perf_counter()
-            r = e.run_batch(b)
-            wall_ms += (time.perf_counter() - tw) * 1e3
-            s1 = e.stats()
-            dev_ms += s1["last_batch_ms"]
-            match_ms += s1["last_match_ms"]
-            matches += int(r.counts.sum())
-            alg += s1["alg_bytes"] - s0["alg_bytes"]
-            launches += s1["kernel_launches"] - s0["kernel_launches"]
-            h2d += b.nbytes
-            d2h += r.tuples.nbytes + r.counts.nbytes + r.signs.nbytes
-            if args.verbose:
-                print(f"  engine {qids}: dev {s1['last_batch_ms']:.2f} ms match {s1['last_match_ms']:.2f} ms "
-                      f"upd {s1['last_update_ms']:.2f} ms filter {s1['last_filter_ms']:.2f} ms wall {(time.perf_counter() - tw) * 1e3:.1f} ms "
-                      f"matches {int(r.counts.sum())} per-query {r.counts.sum(axis=1).tolist()} "
-                      f"seeds {s1['seeds'] - s0['seeds']} donations {s1['donations'] - s0['donations']} "
-                      f"listed {r.listed}", file=sys.stderr, flush=True)
-        return dev_ms, wall_ms, match_ms, matches, alg, launches, h2d, d2h
-
     for b in batches[:args.warmup]:
-        step(b)
-    rows = []
+        e.run_batch(b)
     sampler = ClockSampler(dev)
     if rank == 0:
         sampler.start()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
+    rows = []
     for b in batches[args.warmup:args.warmup + args.steps]:
         flush.zero_()
         torch.cuda.synchronize()
-        rows.append(step(b))
+        s0 = e.stats()
+        tw = time.perf_counter()
+        r = e.run_batch(b)
+        wall = (time.perf_counter() - tw) * 1e3
+        s1 = e.stats()
+        rows.append((s1["last_batch_ms"], wall, s1["last_match_ms"], int(r.counts.sum()),
+                     s1["alg_bytes"] - s0["alg_bytes"], s1["kernel_launches"] - s0["kernel_launches"],
+                     s1["donations"] - s0["donations"], s1["steals"] - s0["steals"]))
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     clocks = sampler.stop() if rank == 0 else None
-    R = np.array([r[:6] for r in rows], dtype=np.float64)
+    R = np.array(rows, dtype=np.float64)
     dev_ms, wall_ms, match_ms = R[:, 0].sum(), R[:, 1].sum(), R[:, 2].sum()
     matches = int(R[:, 3].sum())
-    alg = float(R[:, 4].sum())
-    launches = int(R[:, 5].sum())
-    h2d = int(sum(r[6] for r in rows) / len(rows))
-    d2h = int(sum(r[7] for r in rows) / len(rows))
     if world > 1:
         dev_ms, wall_ms, matches = combine_over_ranks(dev_ms, wall_ms, matches, "cuda")
     if rank != 0:
         return None
     peak, peak_kind = _peaks()
-    upd = sum(len(b) for b in batches[args.warmup:args.warmup + args.steps]) * world
-    lat = np.sort(R[:, 1])
+    alg = float(R[:, 4].sum())
     achieved = alg / 1e9 / (match_ms / 1e3) if match_ms > 0 else 0.0
-    line = {
-        "metric": "delta_matches_per_sec",
-        "value": matches / (dev_ms / 1e3) if dev_ms > 0 else 0.0,
-        "unit": "matches/s",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": dev_ms / args.steps,
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "u32",
-        "data": "synthetic (seeded Chung-Lu graph, random-walk queries, generated update stream)",
-        "config": {"workload": f"config2: Chung-Lu gamma=2.1, |V|=2^{20 + args.scale}, |E|=2^{24 + args.scale}, "
-                               "16 Zipf(1.2) labels, three 8-vertex queries, batches of 4096 (50/50)",
-                   "form": args.form, "listing": bool(args.list), "filter": args.filter,
-                   "tuned": {k: engines[0][0].get_option(getattr(d, "OPT_" + k.upper()))
-                             for k in ("warps_per_sm", "split_min", "donate_depth")}, "parallelism": f"replicas x{world}",
-                   "l2": "256 MiB buffer written between timed batches"},
-        "updates_per_sec": upd / (dev_ms / 1e3) if dev_ms > 0 else 0.0,
-        "matches": matches,
-        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-        "e2e": {"value": matches / (wall_ms / 1e3) if wall_ms > 0 else 0.0, "unit": "matches/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "updates_per_sec": upd / (wall_ms / 1e3) if wall_ms > 0 else 0.0},
-        "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "k_match", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                     "alg_bytes_per_step": alg / args.steps},
-        "clocks": clocks,
-        "gen_seconds": gen_s,
-    }
-    if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w, batches, args.warmup)
-    return line
-
-
-def summarize(lat_ms, matches, updates, span_s):
-    lat = np.sort(np.asarray(lat_ms))
-    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "matches_per_sec": matches / span_s, "updates_per_sec": updates / span_s, "span_s": span_s,
-            "matches": int(matches)}
-
-
-def run_churn(e, arrivals, batch_list, live, pool):
-    """Poisson batches; every 4th arrival also registers a pool query or
-    retires a live one (alternately, keeping at least 4 live), through
-    the serving loop's queue.  Admission waits are timed per ticket."""
-    import random
-    rnd = random.Random(4)
-    bids, tickets, lock = [], [], threading.Lock()
-    counts = {"registrations": 0, "retirements": 0}
-    base = time.perf_counter()
-
-    def submitter():
-        for k, (a, b) in enumerate(zip(arrivals, batch_list)):
-            now = time.perf_counter() - base
-            if now < a:
-                time.sleep(a - now)
-            if k % 4 == 3:
-                with lock:
-                    retire = (k // 4) % 2 == 1 and len(live) > 4
-                    victim = live.pop(rnd.randrange(len(live))) if retire else None
-                if retire:
-                    e.retire_async(victim)
-                    counts["retirements"] += 1
-                else:
-                    tickets.append((e.register_async(pool[(k // 4) % len(pool)]), time.perf_counter()))
-                    counts["registrations"] += 1
-            bids.append(e.submit(b))
-
-    waits = []
-
-    def admitter():  # admission outcome of each registration, in order
-        k = 0
-        while k < len(tickets) or th.is_alive():
-            if k >= len(tickets):
-                time.sleep(0.001)
-                continue
-            t, t_sub = tickets[k]
-            qid = e.admission(t, 60_000)
-            waits.append((time.perf_counter() - t_sub) * 1e3)
-            if qid is not None:
-                with lock:
-                    live.append(qid)
-            k += 1
-
-    th = threading.Thread(target=submitter)
-    th.start()
-    ta = threading.Thread(target=admitter)
-    ta.start()
-    lat, matches, upd = [], 0, 0
-    for k in range(len(batch_list)):
-        while len(bids) <= k:
-            time.sleep(0.0002)
-        t = e.timing(bids[k])
-        r = e.results(bids[k])
-        lat.append(t["total_ms"])
-        matches += int(r.counts.sum())
-        upd += r.num_updates
-    th.join()
-    ta.join()
-    out = summarize(lat, matches, upd, time.perf_counter() - base)
-    out.update(counts)
-    out["admission_wait_ms"] = {"p50": float(np.median(waits)) if waits else None,
-                                "max": float(max(waits)) if waits else None}
-    out["live_queries_at_end"] = e.stats()["live_queries"]
-    return out
-
-
-def run_serve(args):
-    """Serving comparison on the config-4 stream (R-MAT, 32 uniform labels,
-    lognormal batch sizes with median 512, 60% inserts): the same requests
-    through three forms, each from the same initial graph.
-      plain:   one engine per query, one launch per query per batch, in turn;
-      batched: one engine, all queries in one launch per batch;
-      served:  one engine with the serving loop (continuous batching) and
-               CUDA-graph replay of each device batch.
-    Phase 1 (burst): every request at t=0 -> throughput.  Phase 2 (the next
-    requests): Poisson arrivals at 70% of the batched form's burst request
-    rate -> p50 / p99 latency from arrival to results readable on the host.
-    Phase 3 (served form only, the next requests): the same arrivals with
-    query registrations and retirements through the serving loop's queue."""
-    import torch
-
-    import dsm_b200 as d
-    torch.cuda.set_device(0)
-    K = args.serve_requests
-    scale = args.scale if args.scale else -6
-    t0 = time.time()
-    w = d.Workload(4, scale_log2=scale, num_batches=3 * K)
-    gen_s = time.time() - t0
-    reqs = list(w.batches())[:3 * K]
-    burst, poisson, churn = reqs[:K], reqs[K:2 * K], reqs[2 * K:]
-    # 8-10-vertex random-walk queries through the R-MAT hubs carry up to
-    # 10^11 embeddings per request at this scale; the serving comparison uses
-    # the pool's queries of at most 7 vertices
-    qs = [q for q in w.queries if q.nv <= 7][:args.serve_queries]
-    print(f"[serve] workload in {gen_s:.1f} s: {w.nv} vertices, {len(w.edges)} edges, {len(qs)} queries, "
-          f"request sizes median {int(np.median([len(r) for r in reqs]))} max {max(len(r) for r in reqs)}",
-          file=sys.stderr, flush=True)
-
-    def engine(qlist, graph=False):
-        e = d.Engine(0)
-        e.set_option(d.OPT_LIST, args.list)
-        e.set_option(d.OPT_GRAPH, int(graph))
-        e.load_graph_edges(w.nv, w.labels, w.edges)
-        return e, [e.register(q) for q in qlist]
-
-    def run_sync(engines, arrivals, batch_list):
-        """One request at a time, in arrival order, through every engine."""
-        lat, matches, upd = [], 0, 0
-        torch.cuda.synchronize()
-        base = time.perf_counter()
-        for a, b in zip(arrivals, batch_list):
-            now = time.perf_counter() - base
-            if now < a:
-                time.sleep(a - now)
-            for e, _ in engines:
-                r = e.run_batch(b)
-                matches += int(r.counts.sum())
-            lat.append((time.perf_counter() - base - a) * 1e3)
-            upd += len(b)
-        return summarize(lat, matches, upd, time.perf_counter() - base)
-
-    def run_served(e, arrivals, batch_list):
-        bids = []
-        base = time.perf_counter()
-
-        def submitter():
-            for a, b in zip(arrivals, batch_list):
-                now = time.perf_counter() - base
-                if now < a:
-                    time.sleep(a - now)
-                bids.append(e.submit(b))
-
-        th = threading.Thread(target=submitter)
-        th.start()
-        lat, matches, upd, merged = [], 0, 0, []
-        for k in range(len(batch_list)):
-            while len(bids) <= k:
-                time.sleep(0.0002)
-            t = e.timing(bids[k])
-            r = e.results(bids[k])
-            lat.append(t["total_ms"])
-            merged.append(t["merged_requests"])
-            matches += int(r.counts.sum())
-            upd += r.num_updates
-        th.join()
-        out = summarize(lat, matches, upd, time.perf_counter() - base)
-        out["mean_requests_per_device_batch"] = float(np.mean(merged))
-        return out
-
-    arms = {}
-    sampler = ClockSampler(0)
-    sampler.start()
-    # batched first: its burst rate sets the Poisson rate
-    e, _ = engine(qs)
-    arms["batched"] = {"burst": run_sync([(e, None)], np.zeros(K), burst)}
-    rate = 0.7 * K / arms["batched"]["burst"]["span_s"]
-    arrivals = np.cumsum(np.random.default_rng(4).exponential(1.0 / rate, K))
-    arms["batched"]["poisson"] = run_sync([(e, None)], arrivals, poisson)
-    e.close()
-    print(f"[serve] batched done; Poisson rate {rate:.1f} requests/s", file=sys.stderr, flush=True)
-    e, ids = engine(qs, graph=True)  # the served form replays its batch segments as CUDA graphs
-    e.serve_start(args.serve_merge)
-    arms["served"] = {"burst": run_served(e, np.zeros(K), burst), "poisson": run_served(e, arrivals, poisson)}
-    # served only: the same arrivals with query churn (other forms would need
-    # engines to come and go; the live set differs, so no cross-form check)
-    pool = [q for q in w.queries if q.nv <= 7][args.serve_queries:] or qs
-    arms["served"]["churn"] = run_churn(e, arrivals, churn, list(ids), pool)
-    e.serve_stop()
-    e.close()
-    print("[serve] served done", file=sys.stderr, flush=True)
-    engines = [engine([q]) for q in qs]
-    arms["plain"] = {"burst": run_sync(engines, np.zeros(K), burst), "poisson": run_sync(engines, arrivals, poisson)}
-    for e, _ in engines:
-        e.close()
-    clocks = sampler.stop()
-    for k in ("batched", "served", "plain"):
-        assert arms[k]["burst"]["matches"] == arms["batched"]["burst"]["matches"], "forms disagree"
-        assert arms[k]["poisson"]["matches"] == arms["batched"]["poisson"]["matches"], "forms disagree"
-    sv = arms["served"]["poisson"]
-    return {
-        "metric": "served_p99_batch_latency_ms", "value": sv["p99_ms"], "unit": "ms", "n_gpus": 1,
-        "higher_is_better": False, "dtype": "u32", "data": "synthetic (seeded R-MAT graph, generated stream)",
-        "config": {"workload": f"config4 stream on R-MAT(0.57,0.19,0.19) |V|=2^{24 + scale}, "
-                               f"|E|=2^{28 + scale}, 32 uniform labels, {len(qs)} queries of 4-7 vertices "
-                               f"(the first of the 64-query pool of 4-10 vertices with at most 7), "
-                               f"lognormal request sizes (median 512), 60% inserts",
-                   "requests_per_phase": K, "poisson_rate_per_s": rate, "listing": bool(args.list),
-                   "max_merge_updates": args.serve_merge or 65536},
-        "arms": arms, "clocks": clocks, "gen_seconds": gen_s,
-    }
-
-
-def _oracle_sample(streams, batch, target_s, threads):
-    """Counts (all host threads) on the batch's first updates, 16 at a time,
-    until target_s seconds of matching; then the rest of the batch is applied
-    to the graphs without matching.  Returns (matches, seconds, updates)."""
-    matches, secs, pos = 0, 0.0, 0
-    while pos < len(batch) and secs < target_s:
-        chunk = batch[pos:pos + 16]
-        for st in streams:
-            t = time.perf_counter()
-            _, c, _ = st.apply(chunk, listed=False, threads=threads)
-            secs += time.perf_counter() - t
-            matches += int(c.sum())
-        pos += len(chunk)
-    for st in streams:
-        st.apply_graph(batch[pos:])
-    return matches, secs, pos
-
-
-def _oracle_streams(w, warm):
-    from oracle import oracle as orc
-    streams = [orc.Stream(w.nv, w.labels, w.edges, q.labels, q.offsets, q.nbrs) for q in w.queries]
-    for b in warm:  # the graph state the first timed batch sees
-        for st in streams:
-            st.apply_graph(b)
-    return streams
-
-
-def cpu_baseline(w, batches, warmup, target_s=10.0):
-    """The oracle (CPU restatement of the same per-update matching, exact
-    counts, all host threads) on a prefix of the first timed batch, on the
-    graph state that batch sees on the GPU."""
-    threads = os.cpu_count() or 1
-    streams = _oracle_streams(w, batches[:warmup])
-    matches, secs, n = _oracle_sample(streams, batches[warmup], target_s, threads)
-    return {"value": matches / secs if secs > 0 else 0.0, "unit": "matches/s", "cores": threads, "kind": "port",
-            "sample": f"first {n} updates of the first timed batch x {len(w.queries)} queries, counts, "
-                      f"{threads} threads", "seconds": secs}
-
-
-def run_reference(args, rank):
-    """The CPU arm: each step = a bounded prefix of that step's batch (about
-    args.ref_step_s seconds of matching on all host threads), counts."""
-    if rank != 0:
-        return None
-    w = make_workload(args.steps, args.warmup, args.scale)
-    batches = list(w.batches())
-    threads = os.cpu_count() or 1
-    streams = _oracle_streams(w, batches[:args.warmup])
-    secs = matches = upd = 0
-    for b in batches[args.warmup:args.warmup + args.steps]:
-        m, s, n = _oracle_sample(streams, b, args.ref_step_s, threads)
-        matches, secs, upd = matches + m, secs + s, upd + n
-    v = matches / secs if secs > 0 else 0.0
-    return {"impl": "reference", "metric": "delta_matches_per_sec", "value": v, "unit": "matches/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+    upd = sum(len(b) for b in batches[args.warmup:args.warmup + args.steps]) * world
+    line = {"metric": "delta_matches_per_sec", "value": matches / (dev_ms / 1e3), "unit": "matches/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic", "config": {"workload": "config2 (as the GPU arm)", "form": "CPU, per update"},
-            "cpu_baseline": {"value": v, "unit": "matches/s", "cores": threads, "kind": "port",
-                             "sample": f"{upd} updates: a prefix of each timed batch (about {args.ref_step_s} s "
-                                       f"each) x {len(w.queries)} queries, counts"},
-            "e2e": {"value": v, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic (seeded Chung-Lu graph, random-walk queries, generated update stream)",
+            "config": {"workload": f"config2: Chung-Lu gamma=2.1, |V|=2^{20 + args.scale}, |E|=2^{24 + args.scale}, "
+                                   "16 Zipf(1.2) labels, three 8-vertex queries, batches of 4096 (50/50)",
+                       "listing": False, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB buffer written between timed batches",
+                       "tuned": {k: e.get_option(getattr(d, "OPT_" + k.upper()))
+                                 for k in ("warps_per_sm", "split_min", "donate_depth")}},
+            "updates_per_sec": upd / (dev_ms / 1e3), "matches": matches,
+            "latency_ms": {"p50": float(np.percentile(R[:, 1], 50)), "p99": float(np.percentile(R[:, 1], 99))},
+            "e2e": {"value": matches / (wall_ms / 1e3), "unit": "matches/s",
+                    "h2d_bytes_per_step": int(np.mean([b.nbytes for b in batches[args.warmup:]])),
+                    "d2h_bytes_per_step": int(len(w.queries) * 4096 * 8 + 4096)},
+            "gpu_launches": int(R[:, 5].sum()), "donations": int(R[:, 6].sum()), "steals": int(R[:, 7].sum()),
+            "roofline": {"bound": "hbm", "kernel": "k_match", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None},
+            "clocks": clocks, "gen_seconds": gen_s}
+    e.close()
+    return line
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="batched", choices=["batched", "plain"])
-    # config 2's tree and one-cycle queries give 10^6..10^9 embeddings per batch
-    # at full size: the default measures exact counts (listing is covered by
-    # the parity tests); --list 1 lists and sorts them as well
-    ap.add_argument("--list", type=int, default=0)
-    ap.add_argument("--filter", type=int, default=0, help="candidate filter: 0 none, 1 LDF+NLF, 2 cluster encoding")
-    ap.add_argument("--verbose", action="store_true")
-    ap.add_argument("--autotune", type=int, default=1, help="1: tune the matcher launch on the first warm-up batch")
+    ap.add_argument("--mode", default="serve", choices=["serve", "step"])
     ap.add_argument("--scale", type=int, default=0, help="log2 shrink of the graph (0 = config size)")
-    ap.add_argument("--ref-step-s", type=float, default=5.0, help="CPU arm: seconds of matching per step")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="step", choices=["step", "serve"],
-                    help="serve: served vs batched vs plain on the config-4 request stream")
-    ap.add_argument("--serve-requests", type=int, default=200)
-    ap.add_argument("--serve-queries", type=int, default=16)
+    ap.add_argument("--queries", type=int, default=64, help="queries registered at the start (of the 64-query pool)")
+    ap.add_argument("--work-limit", type=int, default=1 << 26,
+                    help="partial embeddings one (query, update) search may generate")
+    ap.add_argument("--query-list-limit", type=int, default=1 << 22,
+                    help="tuples one query may list per device batch")
+    ap.add_argument("--load", type=float, default=0.7, help="Poisson rate / batched burst rate")
     ap.add_argument("--serve-merge", type=int, default=0)
+    ap.add_argument("--autotune", type=int, default=1)
+    ap.add_argument("--cpu-s", type=float, default=15.0, help="seconds of CPU matching for cpu_baseline")
+    ap.add_argument("--ref-s", type=float, default=60.0, help="reference arm: seconds of CPU matching")
+    ap.add_argument("--ref-host-s", type=float, default=60.0, help="reference arm: seconds of updateHostGraph")
+    ap.add_argument("--no-ref-host", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    if args.mode == "serve":
-        print(json.dumps(run_serve(args)), flush=True)
-        return
     if args.impl == "reference":
         # CPU arm: rank 0 alone runs; other ranks exit without work
         line = run_reference(args, rank)
@@ -548,7 +665,19 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = True
     try:
-        line = run_ours(args, rank, world)
+        if args.mode == "step":
+            line = run_step(args, rank, world)
+        else:
+            line = run_serve(args, rank, world)
+            if world > 1:  # replicas: the slowest rank's time, everyone's matches
+                import torch
+                dm, wm, mt = combine_over_ranks(line["forms"]["served"]["device_ms_burst"],
+                                                line["forms"]["served"]["burst"]["span_s"] * 1e3,
+                                                line["matches"], "cuda")
+                line["value"] = mt / (dm / 1e3)
+                line["e2e"]["value"] = mt / (wm / 1e3)
+                if rank != 0:
+                    line = None
         if line is not None:
             print(json.dumps(line), flush=True)
     finally:

@@ -78,6 +78,7 @@ _sig("dsm_graph_info", C.c_int, P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
 _sig("dsm_graph_apply", C.c_int, P, P, C.c_uint32)
 _sig("dsm_query_register", C.c_int, P, u32p, u32p, u32p, C.c_uint32, C.POINTER(C.c_uint32))
 _sig("dsm_query_retire", C.c_int, P, C.c_uint32)
+_sig("dsm_query_live", C.c_int, P, P, C.c_uint32, C.POINTER(C.c_uint32))
 _sig("dsm_query_order", C.c_int, P, C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p)
 _sig("dsm_query_filter", C.c_int, P, C.c_uint32, P, P)
 _sig("dsm_query_plan", C.c_int, u32p, u32p, u32p, C.c_uint32, P, P, P, P, P)
@@ -366,6 +367,13 @@ class Engine:
 
     def retire(self, qid):
         self._ck(lib.dsm_query_retire(self._h, qid))
+
+    def live_queries(self):
+        n = C.c_uint32()
+        self._ck(lib.dsm_query_live(self._h, None, 0, C.byref(n)))
+        ids = np.zeros(max(n.value, 1), np.uint32)
+        self._ck(lib.dsm_query_live(self._h, ids.ctypes.data, len(ids), C.byref(n)))
+        return ids[:n.value].tolist()
 
     def order(self, qid, u, v, nq):
         o = np.zeros(nq, np.uint32)

@@ -180,6 +180,21 @@ int dsm_graph_export(dsm_engine *e, uint32_t *offsets, uint32_t *nbrs, uint64_t 
   return e->e.export_graph(offsets, nbrs, num_entries);
 }
 
+int dsm_query_live(dsm_engine *e, uint32_t *qids, uint32_t cap, uint32_t *num) {
+  ENGINE_OR_ARG(e);
+  if (!num) return DSM_ERR_ARG;
+  Engine &E = e->e;
+  std::lock_guard<std::mutex> lk(E.mu);
+  uint32_t n = 0;
+  for (uint32_t id = 0; id < E.slots.size(); ++id)
+    if (E.slots[id].live) {
+      if (qids && n < cap) qids[n] = id;
+      ++n;
+    }
+  *num = n;
+  return DSM_OK;
+}
+
 int dsm_graph_apply(dsm_engine *e, const dsm_update *ups, uint32_t n) {
   ENGINE_OR_ARG(e);
   if (!ups && n) return DSM_ERR_ARG;

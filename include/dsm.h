@@ -144,6 +144,9 @@ int dsm_query_register(dsm_engine *e, const uint32_t *q_offsets, const uint32_t 
                        const uint32_t *q_labels, uint32_t nq, uint32_t *qid);
 /* Ends matching for qid; a later registration may reuse the id. */
 int dsm_query_retire(dsm_engine *e, uint32_t qid);
+/* The ids of the registered queries, ascending: *num = their number; up to
+ * cap of them are written to qids (which may be NULL to learn *num). */
+int dsm_query_live(dsm_engine *e, uint32_t *qids, uint32_t cap, uint32_t *num);
 /* Matching order for ordered query edge (u, v): order[p] = query vertex at
  * position p; bn_mask[p] = positions < p adjacent to it (OrderCPU's
  * v_orders / backward_neighbors, order.h:78-111). */

@@ -16,6 +16,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <fstream>
@@ -948,6 +949,11 @@ struct orc_file {
 };
 struct orc_stream {
   Stream s;
+  std::unique_ptr<Pool> pool;  // kept between calls (probe is called per update)
+  Pool &threads(int n) {
+    if (!pool || (int)pool->th.size() != n) pool.reset(new Pool(n));
+    return *pool;
+  }
 };
 
 extern "C" {
@@ -1120,7 +1126,7 @@ int orc_stream_apply(orc_stream *h, uint32_t n, const uint32_t *ups, int list) {
 int orc_stream_apply_mt(orc_stream *h, uint32_t n, const uint32_t *ups, int list, int threads) {
   Stream &S = h->s;
   if (threads < 1) threads = (int)std::max(1u, std::thread::hardware_concurrency());
-  Pool pool(threads);
+  Pool &pool = h->threads(threads);
   S.sign.assign(n, 0);
   S.count.assign(n, 0);
   S.tuples.clear();
@@ -1201,9 +1207,8 @@ uint64_t orc_stream_probe(orc_stream *h, uint32_t op, uint32_t a, uint32_t b, in
     la.insert(std::lower_bound(la.begin(), la.end(), b), b);
     lb.insert(std::lower_bound(lb.begin(), lb.end(), a), a);
   }
-  Pool pool(threads);
   std::vector<uint32_t> none;
-  const uint64_t c = match_edge_mt(S, a, b, false, none, pool, threads);
+  const uint64_t c = match_edge_mt(S, a, b, false, none, h->threads(threads), threads);
   if (op == 1) {
     la.erase(std::lower_bound(la.begin(), la.end(), b));
     lb.erase(std::lower_bound(lb.begin(), lb.end(), a));

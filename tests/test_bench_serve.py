@@ -1,6 +1,6 @@
-"""Host logic of bench.py's serving comparison, on a stand-in engine that
-honours the same call contract (submit / timing / results, asynchronous
-registration and retirement, admission).  No GPU."""
+"""Host logic of bench.py's serving comparison on stand-in engines that honour
+the engine's call contract (submit / timing / results, registration and
+retirement, graph-only apply), and its CPU sample on a tiny workload.  No GPU."""
 import os
 import sys
 import threading
@@ -14,60 +14,118 @@ import bench  # noqa: E402
 
 
 class StandIn:
-    def __init__(self, live):
+    """A 'graph' of undirected edges; a batch reports sign +1 / -1 for each
+    effective insert / delete (0 for a no-op) and count 2 per live query."""
+
+    def __init__(self, edges, nq):
         self.lock = threading.Lock()
-        self.live = set(live)
-        self.sizes, self.tickets = {}, {}
-        self.next_bid, self.next_ticket, self.next_qid = 1, 1, 100
-        self.retired = []
+        self.edges = {tuple(sorted(map(int, e))) for e in edges}
+        self.live = list(range(nq))
+        self.next_bid, self.pending = 1, {}
+        self.calls = []
+
+    def _apply(self, b):
+        signs = np.zeros(len(b), np.int8)
+        for i, (op, a, c, _) in enumerate(b):
+            k = tuple(sorted((int(a), int(c))))
+            if a == c:
+                continue
+            if op == 1 and k not in self.edges:
+                self.edges.add(k)
+                signs[i] = 1
+            elif op == 0 and k in self.edges:
+                self.edges.remove(k)
+                signs[i] = -1
+        return signs
 
     def submit(self, b):
         with self.lock:
+            signs = self._apply(b)
             bid = self.next_bid
             self.next_bid += 1
-            self.sizes[bid] = len(b)
+            counts = np.full((len(self.live), len(b)), 2, np.uint64)
+            if len(b):
+                counts[0, 0] |= np.uint64(1 << 63)  # one flagged pair per batch
+            self.pending[bid] = SimpleNamespace(counts=counts, signs=signs, num_updates=len(b),
+                                                tuples=np.zeros(0, np.uint32))
             return bid
 
     def timing(self, bid):
-        return {"total_ms": 1.0 + bid % 3}
+        return {"total_ms": 1.0, "device_ms": 2.0, "merged_requests": 1}
 
     def results(self, bid):
-        n = self.sizes.pop(bid)
-        return SimpleNamespace(counts=np.full((1, n), 2, np.uint64), num_updates=n)
+        return self.pending.pop(bid)
 
-    def register_async(self, q):
+    def register(self, q):
         with self.lock:
-            t = self.next_ticket
-            self.next_ticket += 1
-            self.tickets[t] = self.next_qid
-            self.live.add(self.next_qid)
-            self.next_qid += 1
-            return t
+            qid = min(set(range(len(self.live) + 1)) - set(self.live))
+            self.live.append(qid)
+            self.live.sort()
+            return qid
 
-    def retire_async(self, qid):
+    register_async = register
+
+    def retire(self, qid):
         with self.lock:
-            assert qid in self.live, "retired a query that is not live"
             self.live.remove(qid)
-            self.retired.append(qid)
-            return 0
 
-    def admission(self, t, timeout_ms):
-        return self.tickets[t]
+    retire_async = retire
 
-    def stats(self):
-        return {"live_queries": len(self.live)}
+    def live_queries(self):
+        return list(self.live)
+
+    def apply_graph(self, u):
+        self._apply(u)
 
 
-def test_churn_phase_accounting():
-    e = StandIn(range(6))
-    n = 40
-    out = bench.run_churn(e, np.linspace(0.0, 0.04, n), [np.zeros((5, 4), np.uint32)] * n, list(range(6)), ["q"])
-    assert out["registrations"] + out["retirements"] == n // 4
-    assert out["retirements"] > 0 and out["registrations"] > 0
-    assert out["matches"] == 2 * 5 * n and out["updates_per_sec"] > 0
-    assert out["live_queries_at_end"] == 6 + out["registrations"] - out["retirements"]
-    assert out["admission_wait_ms"]["p50"] is not None
-    assert not e.sizes  # every batch's results were read
+def _stream(seed=1, n=30, size=20, nv=40):
+    rng = np.random.default_rng(seed)
+    edges = rng.integers(0, nv, (60, 2))
+    reqs = []
+    for _ in range(n):
+        b = np.zeros((size, 4), np.uint32)
+        b[:, 0] = rng.random(size) < 0.6
+        b[:, 1:3] = rng.integers(0, nv, (size, 2))
+        reqs.append(b)
+    return edges, reqs
+
+
+def test_churn_schedule():
+    ev = bench.churn_schedule(100, 8, 64)
+    kinds = [e[0][0] for e in ev if e]
+    assert kinds[:4] == ["reg", "ret", "reg", "ret"] and kinds.count("reg") == 13
+    rets = [e[0][1] for e in ev if e and e[0][0] == "ret"]
+    assert len(set(rets)) == len(rets) and len(rets) <= 7  # each initial query retires at most once
+    assert ev == bench.churn_schedule(100, 8, 64)  # deterministic
+
+
+def test_forms_and_restore():
+    """A sync run and a served run of the same requests record the same
+    per-request outcomes; restore() puts the initial graph and queries back."""
+    edges, reqs = _stream()
+    events = bench.churn_schedule(len(reqs), 6, 10)
+    pool = ["q"] * 10
+    e = StandIn(edges, 6)
+    start = set(e.edges)
+    ids = list(range(6))
+    a = bench.FormRun(len(reqs))
+    bench.run_sync(e, reqs, np.zeros(len(reqs)), events, pool, ids, 0, a)
+    again = bench.restore(e, reqs, a.signs, ["q"] * 6)
+    assert e.edges == start and again == ids
+    b = bench.FormRun(len(reqs))
+    bench.run_served(e, reqs, np.linspace(0, 0.01, len(reqs)), events, pool, ids, 0, b)
+    assert np.array_equal(a.matches, b.matches) and np.array_equal(a.flagged, b.flagged)
+    assert (a.flagged == 1).all()
+    assert all(np.array_equal(x, y) for x, y in zip(a.signs, b.signs))
+
+
+def test_cpu_sample_tiny():
+    import dsm_b200 as d
+    w = d.Workload(4, scale_log2=-12, num_batches=12)
+    reqs = list(w.batches())
+    events = bench.churn_schedule(len(reqs), 4, len(w.queries))
+    out = bench.cpu_sample(w, reqs, 2, 5, w.queries[:4], w.queries, events, 2.0, 1 << 20, threads=2)
+    assert out["kind"] == "port" and out["cores"] == 2 and out["seconds"] > 0
 
 
 def test_summarize():

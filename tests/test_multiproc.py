@@ -52,10 +52,14 @@ def test_reference_arm_under_torchrun():
     port = _free_port()
     r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
                         "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
-                        "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--scale", "-6",
-                        "--ref-step-s", "0.2"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+                        "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--scale", "-8",
+                        "--ref-s", "0.5", "--ref-host-s", "0.5"], capture_output=True, text=True, timeout=600,
+                       cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] >= 0 and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["h2d_bytes_per_step"] == 0
+    # the CPU arm generates its inputs through the oracle library: the engine library stays unloaded
+    assert "libdsm" not in r.stderr
