@@ -423,6 +423,27 @@ int clustering(uint32_t nq, const std::vector<uint32_t> &toff,
   return 0;
 }
 
+// final position of each u (filter.cu:1582-1609): newest valid cluster
+// first, each query vertex at its first position there
+std::vector<uint32_t> pick_positions(const Plan &P, uint32_t nq) {
+  std::vector<uint32_t> pos_of_u(nq, kInvalid);
+  std::vector<char> vis(nq, 0);
+  uint32_t cnt = 0;
+  for (int cid = (int)P.final_cluster; cid >= 0; --cid) {
+    if (!P.valid[cid]) continue;
+    if (cnt == nq) break;
+    for (uint32_t p = P.cl_off[cid]; p < P.cl_off[cid + 1]; ++p) {
+      uint32_t u = P.compact[p];
+      if (!vis[u]) {
+        vis[u] = 1;
+        pos_of_u[u] = p;
+        ++cnt;
+      }
+    }
+  }
+  return pos_of_u;
+}
+
 struct Enc {
   uint32_t nb;
   std::vector<uint32_t> w;
@@ -589,22 +610,7 @@ int cluster_filter_impl(uint32_t nq, const uint32_t *qlabels, const uint32_t *qo
       if (op_combine(cptr)) return -2;
       ++cptr;
     }
-  // final position of each u (filter.cu:1582-1609)
-  pos_of_u.assign(nq, kInvalid);
-  std::vector<char> vis(nq, 0);
-  uint32_t cnt = 0;
-  for (int cid = (int)P.final_cluster; cid >= 0; --cid) {
-    if (!P.valid[cid]) continue;
-    if (cnt == nq) break;
-    for (uint32_t p = P.cl_off[cid]; p < P.cl_off[cid + 1]; ++p) {
-      uint32_t u = P.compact[p];
-      if (!vis[u]) {
-        vis[u] = 1;
-        pos_of_u[u] = p;
-        ++cnt;
-      }
-    }
-  }
+  pos_of_u = pick_positions(P, nq);
   // compact (filter.cu:1692-1749): per-u bitmaps over data vertices.
   uint32_t col = (G.nv + 31) / 32;
   bitmaps.assign((size_t)nq * col, 0);
@@ -1014,6 +1020,37 @@ int orc_cluster_filter(uint32_t nq, const uint32_t *qlabels, const uint32_t *qof
   if (plan_out) std::copy(plan.begin(), plan.begin() + std::min<size_t>(plan.size(), 4096), plan_out);
   if (plan_len_out) *plan_len_out = (uint32_t)(plan.size() / 8);
   return 0;
+}
+
+int orc_cluster_plan(uint32_t nq, const uint32_t *qoff, const uint32_t *qnbr, uint32_t *out, uint32_t cap) {
+  if (nq == 0 || nq > 32) return -2;
+  std::vector<uint32_t> toff, tnbr, tdeg;
+  decycle_impl(nq, qoff, qnbr, toff, tnbr, tdeg);
+  Plan P;
+  if (int rc = clustering(nq, toff, tnbr, tdeg, P)) return rc;
+  std::vector<uint32_t> w{P.num_clusters, P.final_cluster, (uint32_t)P.merge_left.size(),
+                          (uint32_t)P.comb_out.size(), P.num_layers};
+  for (uint32_t c = 0; c < P.num_clusters; ++c) {
+    w.push_back(P.valid[c] ? 1 : 0);
+    w.push_back((uint32_t)P.cl[c].size());
+    w.insert(w.end(), P.cl[c].begin(), P.cl[c].end());
+  }
+  for (size_t k = 0; k < P.merge_left.size(); ++k) {
+    w.push_back(P.merge_left[k]);
+    w.push_back(P.merge_right[k]);
+  }
+  for (size_t k = 0; k < P.comb_out.size(); ++k) {
+    w.push_back(P.comb_out[k]);
+    w.push_back((uint32_t)P.comb_type[k]);
+    w.push_back((uint32_t)P.comb_small[k].size());
+    for (int o : P.comb_small[k]) w.push_back((uint32_t)o);
+  }
+  for (uint32_t l = 0; l <= P.num_layers; ++l) w.push_back(P.layer_off[l]);
+  std::vector<uint32_t> pos = pick_positions(P, nq);
+  w.insert(w.end(), pos.begin(), pos.end());
+  if (w.size() > cap) return -3;
+  std::copy(w.begin(), w.end(), out);
+  return (int)w.size();
 }
 
 int orc_stream_new(uint32_t nv, const uint32_t *labels, uint64_t ne, const uint32_t *edges,

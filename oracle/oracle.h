@@ -80,6 +80,10 @@ int orc_order(uint32_t nq, const uint32_t *qoff, const uint32_t *qnbr,
  * record of 8 words per op: kind (0 encode, 1 merge, 2 combine), cluster,
  * a, b, c, d, e, f (see oracle.cpp). plan_len_out = number of ops.
  * Returns 0, or -2 when the query exceeds the reference's limits. */
+/* The cluster plan alone (vertex cover, clusters, merges, combines, layer
+ * offsets, enc_pos_of_u) of the decycled query, serialised as the reference
+ * harness's ref_cluster_plan does; returns words written or < 0. */
+int orc_cluster_plan(uint32_t nq, const uint32_t *qoff, const uint32_t *qnbr, uint32_t *out, uint32_t cap);
 int orc_cluster_filter(uint32_t nq, const uint32_t *qlabels, const uint32_t *qoff,
                        const uint32_t *qnbr, uint32_t nv, const uint32_t *labels,
                        const uint32_t *off, const uint32_t *nbr, uint32_t *bitmaps,

@@ -38,6 +38,7 @@ for n in ("labels", "offsets", "nbrs", "edges", "batch_sizes", "updates"):
     _sig(f"orc_file_{n}", C.POINTER(C.c_uint32), P)
 _sig("orc_decycle", C.c_int, C.c_uint32, u32p, u32p, u32p, u32p, u32p)
 _sig("orc_order", C.c_int, C.c_uint32, u32p, u32p, C.c_uint32, C.c_uint32, u32p, u32p)
+_sig("orc_cluster_plan", C.c_int, C.c_uint32, u32p, u32p, u32p, C.c_uint32)
 _sig("orc_cluster_filter", C.c_int, C.c_uint32, u32p, u32p, u32p, C.c_uint32, u32p, u32p, u32p, P, P, P, P, P)
 _sig("orc_stream_new", C.c_int, C.c_uint32, u32p, C.c_uint64, u32p, C.c_uint32, u32p, u32p, u32p, C.POINTER(P))
 _sig("orc_stream_free", None, P)
@@ -112,6 +113,16 @@ def order(qoff, qnbr, u, v):
     if lib.orc_order(nq, qoff, qnbr, u, v, o, b):
         raise ValueError("disconnected query")
     return o, b
+
+
+def cluster_plan(qoff, qnbr):
+    """The cluster plan of the decycled query, serialised (see oracle.h)."""
+    nq = len(qoff) - 1
+    out = np.zeros(1 << 16, np.uint32)
+    n = lib.orc_cluster_plan(nq, _u32(qoff), _u32(qnbr), out, len(out))
+    if n < 0:
+        raise ValueError(f"cluster plan failed ({n})")
+    return out[:n].copy()
 
 
 def cluster_filter(qlabels, qoff, qnbr, nv, labels, off, nbr):

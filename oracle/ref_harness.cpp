@@ -13,12 +13,14 @@
 
 #include "cpuGraph.h"
 #include "decycle.h"
+#include "filter.cuh"
+#include "globals.cuh"
+#include "io.cuh"
 #include "order.h"
+#include "structure.cuh"
 
-// The two host globals these sources read (declared in globals.cuh; the
-// reference's globals.cu does not compile on its own).
-uint32_t NUM_VQ = 0;
-uint32_t NUM_EQ = 0;
+// The host globals these sources read (NUM_VQ, NUM_EQ, ...) come from the
+// reference's own globals.cu, linked into the same library.
 
 namespace {
 
@@ -107,6 +109,113 @@ int ref_order(uint32_t nq, uint32_t ne, const uint32_t *edges, uint32_t u, uint3
   }
   return 0;
 }
+
+// ---- cluster-filter plan (filter.cu:23-392, structure.cu:113-135) -------
+// The reference's decycle, then its clustering of the spanning tree
+// (vertex cover, merges, combines, encodingMeta::init), then the position
+// pick of clusterFilter (filter.cu:1582-1609, which sits inside a function
+// that launches kernels, so it is restated here: newest valid cluster first,
+// each query vertex at its first position there).  Serialised into out:
+//   num_clusters, final_cluster_id, merge_count, combine_cnt, num_layers,
+//   per cluster c: valid, size, its query vertices (core first),
+//   per merge: left, right,
+//   per combine: out cluster, type, number of others, the others (ascending),
+//   layer offsets (num_layers + 1),
+//   enc_pos_of_u (nq).
+// Returns the number of words written, or a negative code.
+int ref_cluster_plan(uint32_t nq, uint32_t ne, const uint32_t *edges, uint32_t *out, uint32_t cap) {
+  if (nq == 0 || nq > 16) return -1;
+  cpuGraph g;
+  fill_query(g, nq, ne, edges);
+  NUM_VQ = nq;
+  NUM_EQ = ne;
+  decycle(&g);
+  std::vector<cpuCluster> cl;
+  encodingMeta meta;
+  clustering(&g, cl, &meta);
+  std::vector<uint32_t> w;
+  const uint32_t nc = meta.num_clusters;
+  w.push_back(nc);
+  w.push_back(meta.final_cluster_id);
+  w.push_back(meta.merge_count);
+  w.push_back(meta.combine_cnt);
+  w.push_back(meta.num_layers);
+  for (uint32_t c = 0; c < nc; ++c) {
+    w.push_back(meta.is_a_valid_cluster_[c] ? 1 : 0);
+    w.push_back(cl[c].num_query_us);
+    for (uint32_t k = 0; k < cl[c].num_query_us; ++k) w.push_back(cl[c].query_us_[k]);
+  }
+  for (uint32_t k = 0; k < meta.merge_count; ++k) {
+    w.push_back(meta.merged_cluster_left_[k]);
+    w.push_back(meta.merged_cluster_right_[k]);
+  }
+  for (uint32_t k = 0; k < meta.combine_cnt; ++k) {
+    w.push_back(meta.combine_cluster_out_[k]);
+    w.push_back((uint32_t)meta.combine_type_[k]);
+    w.push_back((uint32_t)meta.combine_clusters_other_[k].size());
+    for (int o : meta.combine_clusters_other_[k]) w.push_back((uint32_t)o);
+  }
+  for (uint32_t l = 0; l <= meta.num_layers; ++l) w.push_back(meta.layer_offsets_[l]);
+  std::vector<uint32_t> pos(nq, 0xFFFFFFFFu);
+  std::vector<char> vis(nq, 0);
+  uint32_t cnt = 0;
+  for (int c = (int)meta.final_cluster_id; c >= 0; --c) {
+    if (!meta.is_a_valid_cluster_[c]) continue;
+    if (cnt == nq) break;
+    for (uint32_t p = meta.cluster_offsets_[c]; p < meta.cluster_offsets_[c + 1]; ++p) {
+      const uint32_t u = meta.query_us_compact_[p];
+      if (!vis[u]) {
+        vis[u] = 1;
+        pos[u] = p;
+        ++cnt;
+      }
+    }
+  }
+  for (uint32_t u = 0; u < nq; ++u) w.push_back(pos[u]);
+  if (w.size() > cap) return -3;
+  std::copy(w.begin(), w.end(), out);
+  return (int)w.size();
+}
+
+// ---- text files (readGraphToCPUDynamic, io.cu:122-252) --------------------
+void *ref_file_read(const char *path, int is_query) {
+  auto *g = new cpuGraph();
+  g->isQuery = is_query != 0;
+  readGraphToCPUDynamic(g, path);
+  return g;
+}
+
+// nv, ne; then the CSR as parsed (off: nv + 1, nbr: 2 ne, labels: nv) and
+// the batches (sizes: one per batch; ups: 4 words per update, op 1 = add).
+void ref_file_sizes(void *h, uint32_t *nv, uint32_t *ne, uint32_t *nbatches, uint32_t *nupdates) {
+  const cpuGraph &g = *static_cast<cpuGraph *>(h);
+  *nv = g.num_v;
+  *ne = g.num_e;
+  *nbatches = (uint32_t)g.batches.size();
+  size_t n = 0;
+  for (const auto &b : g.batches) n += b.size();
+  *nupdates = (uint32_t)n;
+}
+
+void ref_file_export(void *h, uint32_t *off, uint32_t *nbr, uint32_t *labels, uint32_t *sizes, uint32_t *ups) {
+  const cpuGraph &g = *static_cast<cpuGraph *>(h);
+  for (uint32_t v = 0; v <= g.num_v; ++v) off[v] = g.offsets_[v];
+  for (uint64_t k = 0; k < 2ull * g.num_e; ++k) nbr[k] = g.neighbors_[k];
+  for (uint32_t v = 0; v < g.num_v; ++v) labels[v] = g.vLabels_[v];
+  size_t i = 0;
+  for (size_t b = 0; b < g.batches.size(); ++b) {
+    sizes[b] = (uint32_t)g.batches[b].size();
+    for (const change &c : g.batches[b]) {
+      ups[4 * i] = c.add ? 1 : 0;
+      ups[4 * i + 1] = c.src;
+      ups[4 * i + 2] = c.dst;
+      ups[4 * i + 3] = c.labelChange;
+      ++i;
+    }
+  }
+}
+
+void ref_file_free(void *h) { delete static_cast<cpuGraph *>(h); }
 
 // ---- data graph and updateHostGraph (cpuGraph.cpp:521-607) ---------------
 // A data cpuGraph filled as readGraphToCPUDynamic fills it (io.cu:122-252):

@@ -168,3 +168,76 @@ def test_update_host_graph_pins_batch_application():
         print(f"insert+delete of one edge in a batch: reference keeps the edge: {ref_has}")
     finally:
         lib.ref_graph_free(h)
+
+
+@pytest.mark.parametrize("ascending", [True, False])
+def test_cluster_plan_against_reference(ascending):
+    """The oracle's cluster-filter plan against the reference's own code:
+    decycle, then getVertexCover / clustering (filter.cu:23-392) with
+    encodingMeta::init (structure.cu:113-135) -- the clusters in order with
+    their query vertices and validity, every merge and combine, the layer
+    offsets -- and the position pick of clusterFilter (filter.cu:1582-1609),
+    on the fixture's query shape and 60 random queries."""
+    lib = C.CDLL(LIB)
+    u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+    lib.ref_cluster_plan.argtypes = [C.c_uint32, C.c_uint32, u32p, u32p, C.c_uint32]
+    merges = combines = 0
+    for nq, edges in _queries(ascending):
+        flat = np.array(edges, np.uint32).reshape(-1)
+        out = np.zeros(1 << 16, np.uint32)
+        n = lib.ref_cluster_plan(nq, len(edges), flat, out, len(out))
+        assert n > 0
+        qoff, qnbr = _csr_file_order(nq, edges)
+        ours = orc.cluster_plan(qoff, qnbr)
+        assert np.array_equal(ours, out[:n]), (nq, edges)
+        merges += int(out[2])
+        combines += int(out[3])
+    assert merges > 50 and combines > 10  # the plans exercise merges and combines
+
+
+def test_text_parsers_against_reference(tmp_path):
+    """The engine's text reader and the oracle's parser against the
+    reference's readGraphToCPUDynamic (io.cu:122-252) on generated files: the
+    CSR in file order, the labels, and every batch's updates."""
+    import dsm_b200 as d
+    lib = C.CDLL(LIB)
+    lib.ref_file_read.restype = C.c_void_p
+    lib.ref_file_read.argtypes = [C.c_char_p, C.c_int]
+    lib.ref_file_sizes.argtypes = [C.c_void_p] + [C.POINTER(C.c_uint32)] * 4
+    lib.ref_file_export.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+    lib.ref_file_free.argtypes = [C.c_void_p]
+
+    def ref_parse(path, isq):
+        h = lib.ref_file_read(path.encode(), int(isq))
+        try:
+            nv, ne, nb, nu = (C.c_uint32() for _ in range(4))
+            lib.ref_file_sizes(h, C.byref(nv), C.byref(ne), C.byref(nb), C.byref(nu))
+            off = np.zeros(nv.value + 1, np.uint32)
+            nbr = np.zeros(max(2 * ne.value, 1), np.uint32)
+            lab = np.zeros(nv.value, np.uint32)
+            sizes = np.zeros(max(nb.value, 1), np.uint32)
+            ups = np.zeros(max(4 * nu.value, 1), np.uint32)
+            lib.ref_file_export(h, off.ctypes.data, nbr.ctypes.data, lab.ctypes.data, sizes.ctypes.data,
+                                ups.ctypes.data)
+            return dict(offsets=off, nbrs=nbr[:2 * ne.value], labels=lab, batch_sizes=sizes[:nb.value],
+                        updates=ups[:4 * nu.value].reshape(-1, 4))
+        finally:
+            lib.ref_file_free(h)
+
+    for cfg, scale in ((1, 0), (2, -8)):
+        w = d.Workload(cfg, scale_log2=scale, num_batches=4)
+        w.write(str(tmp_path / f"q{cfg}_"), str(tmp_path / f"g{cfg}.in"))
+        files = [(str(tmp_path / f"g{cfg}.in"), False)]
+        files += [(str(tmp_path / f"q{cfg}_{k}.in"), True) for k in range(len(w.queries))]
+        files += [(os.path.join(ROOT, "tests", "golden", n), n.startswith("example_q")) for n in
+                  ("example_q_01.in", "example_g_01.in")]
+        for path, isq in files:
+            assert os.path.exists(path)  # the reference's reader exits the process on a missing file
+            r = ref_parse(path, isq)
+            a = d.TextGraph(path, isq)
+            o = orc.parse(path, isq)
+            for k in ("offsets", "nbrs", "labels", "batch_sizes", "updates"):
+                assert np.array_equal(getattr(a, k), r[k]), (path, k)
+                assert np.array_equal(o[k], r[k]), (path, k)
+            if not isq:
+                assert len(r["updates"]) > 0
