@@ -26,11 +26,13 @@ sorted).  Each (query, update) search is bounded by DSM_OPT_WORK_LIMIT
 every form (and in the oracle); all other counts are exact, and the forms'
 exact match totals and flags must agree request by request.
 
-Phases: W * 16 warm-up requests (untimed; the first tunes the matcher's
-launch shape), then K * 16 requests at once (burst: throughput), then K * 16
+Phases: W * 4 warm-up requests (untimed; the first tunes the matcher's
+launch shape), then K * 4 requests at once (burst: throughput), then K * 4
 requests arriving as a Poisson process at 70 % of the batched form's burst
 request rate (latency from arrival to sorted results readable on the host).
-A step is 16 requests.
+A step is 4 requests.  The work limit (default 2^18 partial embeddings per
+(query, update)) keeps the pool's explosive queries (8-10 vertices through
+R-MAT hubs, up to 10^11 embeddings per request) to a bounded, flagged cost.
 
 Prints one JSON line.  `value` = the served form's exact delta-matches per
 second of device time over the burst (events around each device batch;
@@ -60,7 +62,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-REQ_PER_STEP = 16
+REQ_PER_STEP = 4
 INCOMPLETE = np.uint64(1 << 63)
 
 
@@ -70,6 +72,28 @@ def _peaks():
         d = json.load(open(p))
         return float(d.get("hbm_gbs", 6650.0)), "measured"
     return 6650.0, "fallback"
+
+
+def measure_l2_gbs():
+    """L2 copy bandwidth (read + write bytes per second) measured here: a
+    16 MiB -> 16 MiB copy repeated, both buffers resident in the 126 MB L2,
+    CUDA events around 50 copies after 10 warm ones, best of 5."""
+    import torch
+    a = torch.empty(4 << 20, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    a.fill_(1.0)
+    for _ in range(10):
+        b.copy_(a)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(50):
+            b.copy_(a)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 50 * 2 * a.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    return best
 
 
 class ClockSampler:
@@ -297,6 +321,11 @@ def run_serve(args, rank=0, world=1):
           file=sys.stderr, flush=True)
     e = d.Engine(dev)
     e.set_option(d.OPT_LIST, 1)
+    e.set_option(d.OPT_FILTER, args.filter)
+    if args.pack >= 0:
+        e.set_option(d.OPT_PACK_MAX, args.pack)
+    if args.merge >= 0:
+        e.set_option(d.OPT_MERGE_MAX, args.merge)
     e.set_option(d.OPT_WORK_LIMIT, args.work_limit)
     e.set_option(d.OPT_QUERY_LIST_LIMIT, args.query_list_limit)
     t0 = time.time()
@@ -351,6 +380,8 @@ def run_serve(args, rank=0, world=1):
             again = restore(e, reqs, run.signs, initial)
             assert again == ids, "the initial queries came back with other ids"
     clocks = sampler.stop()
+    tuned = {k: e.get_option(getattr(d, "OPT_" + k.upper()))
+             for k in ("warps_per_sm", "split_min", "donate_depth", "pack_max", "merge_max")}
 
     # the forms must agree request by request
     ref = runs["batched"]
@@ -408,7 +439,8 @@ def run_serve(args, rank=0, world=1):
                                f"60% inserts",
                    "step": f"{REQ_PER_STEP} requests", "listing": True, "work_limit": args.work_limit,
                    "query_list_limit": args.query_list_limit, "poisson_load": args.load,
-                   "poisson_rate_per_s": rate, "parallelism": f"replicas x{world}",
+                   "poisson_rate_per_s": rate, "parallelism": f"replicas x{world}", "filter": args.filter,
+                   "tuned": tuned,
                    "l2": "inputs (2^28-edge graph, ~5 GB of runs) far larger than L2"},
         "updates_per_sec": sv["device_updates_per_sec"],
         "latency_ms": {"p50": sv["poisson"]["p50_ms"], "p99": sv["poisson"]["p99_ms"]},
@@ -550,6 +582,20 @@ def run_reference(args, rank):
 # ---------------------------------------------------------------------------
 # --mode step: config 2, one 4096-update batch per step (counts)
 # ---------------------------------------------------------------------------
+def step_workload(args, nq, bsz):
+    sc = args.scale
+    if args.config == 2:
+        return (f"config2: Chung-Lu gamma=2.1, |V|=2^{20 + sc}, |E|=2^{24 + sc}, 16 Zipf(1.2) labels, "
+                f"three 8-vertex queries, batches of {bsz} (50/50)")
+    if args.config == 3:
+        return (f"config3: the config-2 graph (|V|=2^{20 + sc}), {nq} queries of 4-12 vertices in one launch, "
+                f"batches of {bsz}")
+    if args.config == 5:
+        return (f"config5: R-MAT(0.70,0.12,0.12) |V|=2^{22 + sc}, |E|=2^{27 + sc}, 8 uniform labels, "
+                f"{nq} twelve-vertex cyclic queries (two triangles + a 4-cycle), batches of {bsz} (80% deletes)")
+    return f"config{args.config} at scale 2^{sc}, {nq} queries, batches of {bsz}"
+
+
 def run_step(args, rank, world):
     import torch
 
@@ -557,15 +603,25 @@ def run_step(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     t0 = time.time()
-    w = d.Workload(2, scale_log2=args.scale, num_batches=args.steps + args.warmup)
+    w = d.Workload(args.config, scale_log2=args.scale, num_batches=args.steps + args.warmup)
     gen_s = time.time() - t0
     batches = list(w.batches())
+    if args.batch:
+        batches = [b[:args.batch] for b in batches]
+    queries = w.queries[:args.queries] if args.config != 2 else w.queries
     e = d.Engine(dev)
     e.set_option(d.OPT_LIST, 0)
+    if args.step_work_limit:
+        e.set_option(d.OPT_WORK_LIMIT, args.step_work_limit)
+    e.set_option(d.OPT_FILTER, args.filter)
+    if args.pack >= 0:
+        e.set_option(d.OPT_PACK_MAX, args.pack)
+    if args.merge >= 0:
+        e.set_option(d.OPT_MERGE_MAX, args.merge)
     if args.autotune and args.warmup > 0:
         e.set_option(d.OPT_AUTOTUNE, 1)
     e.load_graph_edges(w.nv, w.labels, w.edges)
-    for q in w.queries:
+    for q in queries:
         e.register(q)
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MiB > L2
     for b in batches[:args.warmup]:
@@ -576,7 +632,7 @@ def run_step(args, rank, world):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    rows = []
+    rows, flagged = [], 0
     for b in batches[args.warmup:args.warmup + args.steps]:
         flush.zero_()
         torch.cuda.synchronize()
@@ -585,7 +641,10 @@ def run_step(args, rank, world):
         r = e.run_batch(b)
         wall = (time.perf_counter() - tw) * 1e3
         s1 = e.stats()
-        rows.append((s1["last_batch_ms"], wall, s1["last_match_ms"], int(r.counts.sum()),
+        c = r.counts
+        exact = int(c[(c & np.uint64(1 << 63)) == 0].sum())
+        flagged += int(((c & np.uint64(1 << 63)) != 0).sum())
+        rows.append((s1["last_batch_ms"], wall, s1["last_match_ms"], exact,
                      s1["alg_bytes"] - s0["alg_bytes"], s1["kernel_launches"] - s0["kernel_launches"],
                      s1["donations"] - s0["donations"], s1["steals"] - s0["steals"]))
     torch.cuda.synchronize()
@@ -607,17 +666,18 @@ def run_step(args, rank, world):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded Chung-Lu graph, random-walk queries, generated update stream)",
-            "config": {"workload": f"config2: Chung-Lu gamma=2.1, |V|=2^{20 + args.scale}, |E|=2^{24 + args.scale}, "
-                                   "16 Zipf(1.2) labels, three 8-vertex queries, batches of 4096 (50/50)",
+            "config": {"workload": step_workload(args, len(queries), len(batches[0])),
+                       "flagged_pairs": flagged, "work_limit": args.step_work_limit,
                        "listing": False, "parallelism": f"replicas x{world}",
                        "l2": "256 MiB buffer written between timed batches",
+                       "filter": args.filter,
                        "tuned": {k: e.get_option(getattr(d, "OPT_" + k.upper()))
-                                 for k in ("warps_per_sm", "split_min", "donate_depth")}},
+                                 for k in ("warps_per_sm", "split_min", "donate_depth", "pack_max", "merge_max")}},
             "updates_per_sec": upd / (dev_ms / 1e3), "matches": matches,
             "latency_ms": {"p50": float(np.percentile(R[:, 1], 50)), "p99": float(np.percentile(R[:, 1], 99))},
             "e2e": {"value": matches / (wall_ms / 1e3), "unit": "matches/s",
                     "h2d_bytes_per_step": int(np.mean([b.nbytes for b in batches[args.warmup:]])),
-                    "d2h_bytes_per_step": int(len(w.queries) * 4096 * 8 + 4096)},
+                    "d2h_bytes_per_step": int(len(queries) * len(batches[-1]) * 8 + len(batches[-1]))},
             "gpu_launches": int(R[:, 5].sum()), "donations": int(R[:, 6].sum()), "steals": int(R[:, 7].sum()),
             "roofline": {"bound": "hbm", "kernel": "k_match", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": None},
@@ -633,15 +693,21 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="serve", choices=["serve", "step"])
+    ap.add_argument("--config", type=int, default=2, choices=[2, 3, 5], help="--mode step: the workload")
+    ap.add_argument("--batch", type=int, default=0, help="--mode step: updates per batch (0: the config's)")
+    ap.add_argument("--step-work-limit", type=int, default=0, help="--mode step: DSM_OPT_WORK_LIMIT (0: none)")
     ap.add_argument("--scale", type=int, default=0, help="log2 shrink of the graph (0 = config size)")
     ap.add_argument("--queries", type=int, default=64, help="queries registered at the start (of the 64-query pool)")
-    ap.add_argument("--work-limit", type=int, default=1 << 26,
+    ap.add_argument("--work-limit", type=int, default=1 << 18,
                     help="partial embeddings one (query, update) search may generate")
     ap.add_argument("--query-list-limit", type=int, default=1 << 22,
                     help="tuples one query may list per device batch")
     ap.add_argument("--load", type=float, default=0.7, help="Poisson rate / batched burst rate")
     ap.add_argument("--serve-merge", type=int, default=0)
     ap.add_argument("--autotune", type=int, default=1)
+    ap.add_argument("--filter", type=int, default=0, help="DSM_OPT_FILTER (0 labels only, 1 LDF+NLF, 2 cluster encoding)")
+    ap.add_argument("--pack", type=int, default=-1, help="DSM_OPT_PACK_MAX before tuning (-1: engine default)")
+    ap.add_argument("--merge", type=int, default=-1, help="DSM_OPT_MERGE_MAX before tuning (-1: engine default)")
     ap.add_argument("--cpu-s", type=float, default=15.0, help="seconds of CPU matching for cpu_baseline")
     ap.add_argument("--ref-s", type=float, default=60.0, help="reference arm: seconds of CPU matching")
     ap.add_argument("--ref-host-s", type=float, default=60.0, help="reference arm: seconds of updateHostGraph")

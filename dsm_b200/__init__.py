@@ -20,7 +20,7 @@ ERR = {1: "PARSE", 2: "OOM", 3: "OVERFLOW", 4: "TIMEOUT", 5: "LIMIT", 6: "ARG", 
 
 OPT_LIST, OPT_FILTER, OPT_RESULT_CAP, OPT_WARPS_PER_SM, OPT_DONATE, OPT_TIMEOUT_MS, OPT_LABEL_QUIRK, OPT_SORT, \
     OPT_LIST_LIMIT, OPT_MEM_BUDGET, OPT_SPLIT_MIN, OPT_DONATE_DEPTH, OPT_AUTOTUNE, OPT_GRAPH, OPT_STALL_TEST, \
-    OPT_PLAIN, OPT_QUERY_LIST_LIMIT, OPT_WORK_LIMIT = range(1, 19)
+    OPT_PLAIN, OPT_QUERY_LIST_LIMIT, OPT_WORK_LIMIT, OPT_PACK_MAX, OPT_FILTER_INCREMENTAL, OPT_MERGE_MAX = range(1, 22)
 INCOMPLETE = np.uint64(1 << 63)  # bit of a count whose search went over DSM_OPT_WORK_LIMIT
 
 if not os.path.exists(LIB_PATH):
@@ -81,6 +81,7 @@ _sig("dsm_query_retire", C.c_int, P, C.c_uint32)
 _sig("dsm_query_live", C.c_int, P, P, C.c_uint32, C.POINTER(C.c_uint32))
 _sig("dsm_query_order", C.c_int, P, C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p)
 _sig("dsm_query_filter", C.c_int, P, C.c_uint32, P, P)
+_sig("dsm_query_filter_state", C.c_int, P, C.c_uint32, P, P, P)
 _sig("dsm_query_plan", C.c_int, u32p, u32p, u32p, C.c_uint32, P, P, P, P, P)
 _sig("dsm_batch_submit", C.c_int, P, P, C.c_uint32, C.POINTER(C.c_uint64))
 _sig("dsm_batch_wait", C.c_int, P, C.c_uint64)
@@ -387,6 +388,16 @@ class Engine:
         vc = np.zeros(nv, np.uint32)
         self._ck(lib.dsm_query_filter(self._h, qid, bm.ctypes.data, vc.ctypes.data))
         return bm.reshape(nq, col), vc
+
+    def filter_state(self, qid, nq, nv):
+        """The resident filter state of query qid after the last batch:
+        bitmaps, LDF+NLF masks, and (full recompute?, vertices recomputed)."""
+        col = (nv + 31) // 32
+        bm = np.zeros(nq * col, np.uint32)
+        vc = np.zeros(nv, np.uint32)
+        info = np.zeros(2, np.uint32)
+        self._ck(lib.dsm_query_filter_state(self._h, qid, bm.ctypes.data, vc.ctypes.data, info.ctypes.data))
+        return bm.reshape(nq, col), vc, (bool(info[0]), int(info[1]))
 
     @staticmethod
     def pack_updates(updates):

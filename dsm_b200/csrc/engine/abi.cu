@@ -94,6 +94,15 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
       if (value < 0 || value > 4) return E.fail(DSM_ERR_ARG, "donation depth 0..4");
       E.donate_depth = (uint32_t)value;
       return DSM_OK;
+    case DSM_OPT_FILTER_INCREMENTAL: E.filter_incremental = value ? 1 : 0; return DSM_OK;
+    case DSM_OPT_MERGE_MAX:
+      if (value < 0 || value > (1 << 16)) return E.fail(DSM_ERR_ARG, "merge threshold 0..2^16 entries");
+      E.merge_max = (uint32_t)value;
+      return DSM_OK;
+    case DSM_OPT_PACK_MAX:
+      if (value < 0 || value > (1 << 20)) return E.fail(DSM_ERR_ARG, "intersection tile 0..2^20 entries");
+      E.pack_max = (uint32_t)value;
+      return DSM_OK;
     case DSM_OPT_AUTOTUNE: E.tune_next = value != 0; return DSM_OK;
     case DSM_OPT_GRAPH: E.use_graph = value ? 1 : 0; return DSM_OK;
     case DSM_OPT_STALL_TEST: E.stall_test = value ? 1 : 0; return DSM_OK;
@@ -133,6 +142,9 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_MEM_BUDGET: *value = (int64_t)E.budget; return DSM_OK;
     case DSM_OPT_SPLIT_MIN: *value = E.split_min; return DSM_OK;
     case DSM_OPT_DONATE_DEPTH: *value = E.donate_depth; return DSM_OK;
+    case DSM_OPT_PACK_MAX: *value = E.pack_max; return DSM_OK;
+    case DSM_OPT_FILTER_INCREMENTAL: *value = E.filter_incremental; return DSM_OK;
+    case DSM_OPT_MERGE_MAX: *value = E.merge_max; return DSM_OK;
     case DSM_OPT_AUTOTUNE: *value = E.tune_next ? 1 : 0; return DSM_OK;
     case DSM_OPT_GRAPH: *value = E.use_graph; return DSM_OK;
     case DSM_OPT_STALL_TEST: *value = E.stall_test; return DSM_OK;
@@ -248,6 +260,11 @@ int dsm_query_order(dsm_engine *e, uint32_t qid, uint32_t u, uint32_t v, uint32_
 int dsm_query_filter(dsm_engine *e, uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us) {
   ENGINE_OR_ARG(e);
   return e->e.query_filter(qid, bitmaps, v_cand_us);
+}
+
+int dsm_query_filter_state(dsm_engine *e, uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us, uint32_t *info) {
+  ENGINE_OR_ARG(e);
+  return e->e.filter_state(qid, bitmaps, v_cand_us, info);
 }
 
 int dsm_query_plan(const uint32_t *q_offsets, const uint32_t *q_nbrs, const uint32_t *q_labels, uint32_t nq,

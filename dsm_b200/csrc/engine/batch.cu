@@ -167,6 +167,8 @@ int Engine::launch_front(Staged &S) {
   }
   // what allocates, synchronises or copies pageable memory runs before the
   // segments, so that each segment can be captured into a CUDA graph
+  if (!(S.match && filter_mode > 0) && d_rinfo.ptr && n)  // the graph changes unfiltered
+    CK(cudaMemsetAsync(d_rinfo.ptr, 1, 1, stream));  // RegionInfo::stale
   if (qd_dirty)
     if ((rc = upload_qd())) return rc;
   if (S.match && (rc = prepare_filters())) return rc;
@@ -238,6 +240,8 @@ int Engine::launch_front(Staged &S) {
   ma.timeout_cycles = (long long)timeout_ms * (long long)clock_khz;
   ma.split_min = split_min;
   ma.donate_depth = donate_depth;
+  ma.pack_max = pack_max;
+  ma.merge_max = merge_max;
   ma.out_seg = (uint32_t *)d_out_seg.ptr;
   ma.out_tup = (uint32_t *)d_out_tup.ptr;
   ma.cap = list_mode ? std::min<unsigned long long>(d_out_seg.bytes / 4, d_out_tup.bytes / 4 / ma.W) : 0;
@@ -266,6 +270,7 @@ int Engine::launch_front(Staged &S) {
     key_append(key, S.match);
     key_append(key, query_gen);
     key_append(key, filter_mode);
+    key_append(key, filter_incremental);
     key_append(key, stall_test);
     key_append(key, h_sched.ptr);
     key_append(key, h_qlisted.ptr);
@@ -447,6 +452,8 @@ int Engine::finish_device(Staged &S) {
       ma.timeout_cycles = (long long)timeout_ms * (long long)clock_khz;
       ma.split_min = split_min;
       ma.donate_depth = donate_depth;
+      ma.pack_max = pack_max;
+      ma.merge_max = merge_max;
       ma.out_seg = (uint32_t *)d_out_seg.ptr;
       ma.out_tup = (uint32_t *)d_out_tup.ptr;
       ma.cap = std::min<unsigned long long>(d_out_seg.bytes / 4, d_out_tup.bytes / 4 / S.W);
@@ -698,10 +705,11 @@ int Engine::compact_arena(uint64_t extra_words) {
 // ---------------------------------------------------------------------------
 // The matcher's result does not depend on its launch shape or on how work is
 // donated, so the batch's own matcher launch is repeated on the same union
-// graph (counts only) for each candidate -- resident blocks per SM x
-// range-split threshold x donation depth -- timed with events, and the
-// fastest becomes the engine's setting.  The first candidate runs twice and
-// its first run is not counted (it warms L2 for all).
+// graph (counts only) for each candidate -- first the intersection tile
+// (packed last level), then resident blocks per SM x range-split threshold x
+// donation depth at the best tile -- timed with events, and the fastest
+// becomes the engine's setting.  The first candidate runs twice and its first
+// run is not counted (it warms L2 for all).
 int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
   Sched *hs = (Sched *)h_sched.ptr;
   CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
@@ -710,12 +718,8 @@ int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
   const unsigned long long nseeds = hs->nseeds;
   struct Cand {
     int bps;
-    uint32_t split, dd;
+    uint32_t split, dd, pack, merge;
   };
-  std::vector<Cand> cands;
-  for (int bps = std::max(1, match_blocks_per_sm - 2); bps <= match_blocks_per_sm; ++bps)
-    for (uint32_t split : {64u, 128u, 512u})
-      for (uint32_t dd : {1u, 2u}) cands.push_back({bps, split, dd});
   auto rearm = [&]() -> int {
     std::memset(hs, 0, sizeof(Sched));
     hs->nseeds = nseeds;
@@ -732,36 +736,67 @@ int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
   MatchArgs t = ma;
   t.list = 0;
   t.cap = 0;
-  float best = 1e30f;
-  Cand bc{blocks / std::max(num_sms, 1), ma.split_min, ma.donate_depth};
   cudaEvent_t e0 = ev_pool[2], e1 = ev_pool[3];
-  for (int k = -1; k < (int)cands.size(); ++k) {
-    const Cand &c = cands[std::max(k, 0)];
-    if (int rc = rearm()) return rc;
-    t.split_min = c.split;
-    t.donate_depth = c.dd;
-    CK(cudaEventRecord(e0, stream));
-    launch_match(t, num_sms * c.bps, stream);
-    ++stats.kernel_launches;
-    CK(cudaEventRecord(e1, stream));
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
-    if (hs->error) break;  // keep the current setting
-    float ms = 0;
-    elapsed(e0, e1, &ms);
-    stats.tune_runs++;
-    if (k >= 0 && ms < best) {
-      best = ms;
-      bc = c;
+  // times each candidate; bc = the fastest (unchanged when a launch reports
+  // an error in the scheduler word: the batch's real launch reports it)
+  bool stop = false;
+  auto sweep = [&](const std::vector<Cand> &cands, bool warm, Cand &bc, float &best) -> int {
+    best = 1e30f;
+    for (int k = warm ? -1 : 0; k < (int)cands.size() && !stop; ++k) {
+      const Cand &c = cands[std::max(k, 0)];
+      if (int rc = rearm()) return rc;
+      t.split_min = c.split;
+      t.donate_depth = c.dd;
+      t.pack_max = c.pack;
+      t.merge_max = c.merge;
+      CK(cudaEventRecord(e0, stream));
+      launch_match(t, num_sms * c.bps, stream);
+      ++stats.kernel_launches;
+      CK(cudaEventRecord(e1, stream));
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      if (hs->error) {
+        stop = true;
+        break;
+      }
+      float ms = 0;
+      elapsed(e0, e1, &ms);
+      stats.tune_runs++;
+      if (k >= 0 && ms < best) {
+        best = ms;
+        bc = c;
+      }
     }
-  }
-  if (best < 1e30f) {
+    return DSM_OK;
+  };
+  const Cand cur{blocks / std::max(num_sms, 1), ma.split_min, ma.donate_depth, ma.pack_max, ma.merge_max};
+  // stage 1: the intersection tile -- packed last level x merge threshold --
+  // at the current launch shape
+  std::vector<Cand> c1;
+  for (uint32_t pk : {0u, 256u, 1024u, 4096u})
+    for (uint32_t mg : {0u, 64u, 256u}) c1.push_back({cur.bps, cur.split, cur.dd, pk, mg});
+  float best1 = 1e30f, best2 = 1e30f;
+  Cand b1 = cur, bc = cur;
+  if (int rc = sweep(c1, true, b1, best1)) return rc;
+  // stage 2: blocks per SM x split threshold x donation depth, at that tile
+  std::vector<Cand> c2;
+  for (int bps = std::max(1, match_blocks_per_sm - 2); bps <= match_blocks_per_sm; ++bps)
+    for (uint32_t split : {64u, 128u, 512u})
+      for (uint32_t dd : {1u, 2u}) c2.push_back({bps, split, dd, b1.pack, b1.merge});
+  bc = b1;
+  if (!stop)
+    if (int rc = sweep(c2, false, bc, best2)) return rc;
+  if (!stop && best2 < 1e30f) {
     warps_per_sm = bc.bps * 8;
     split_min = bc.split;
     donate_depth = bc.dd;
-    stats.tune_best_ms = best;
+    pack_max = bc.pack;
+    merge_max = bc.merge;
+    stats.tune_best_ms = best2;
   }
+  ma.pack_max = pack_max;
+  ma.merge_max = merge_max;
   ma.split_min = split_min;
   ma.donate_depth = donate_depth;
   blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);

@@ -129,7 +129,8 @@ std::vector<DevBuf *> Engine::all_dev_bufs() {
   std::vector<DevBuf *> v = {&d_lab, &d_adj, &d_cap, &d_arena, &d_arena_top, &d_loff, &d_qd, &d_orders,
                              &d_pair_off, &d_pair_ent, &d_upd, &d_bkey, &d_bidx, &d_binfo, &d_gflag,
                              &d_vtp, &d_dkey, &d_dhead, &d_dsel, &d_seeds, &d_sched, &d_jobs,
-                             &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc, &d_hdr, &d_qlisted, &d_segwork};
+                             &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc, &d_hdr, &d_qlisted, &d_segwork,
+                             &d_rinfo, &d_rmark, &d_rlist, &d_rprev};
   for (auto &q : slots) v.push_back(&q.bitmap);
   for (auto &q : slots) v.push_back(&q.filter_scratch);
   for (auto &q : slots) v.push_back(&q.filter_plan);
@@ -252,7 +253,39 @@ int Engine::load_graph(uint32_t nv_, const uint32_t *labels, std::vector<uint64_
   graph_loaded = true;
   label_host.assign(labels, labels + nv_);
   for (auto &q : slots) q.filter_dirty = true;
+  return region_init();
+}
+
+// The incremental filter's region buffers for a new graph: marks cleared,
+// nothing kept from a previous batch, the next filtered batch recomputes
+// every query in full.  List capacity: a quarter of the vertices (at least
+// 2^16); beyond it a region run costs about as much as a full one.
+int Engine::region_init() {
+  const uint32_t cap = std::max<uint32_t>(nv / 4, std::min<uint32_t>(nv, 1u << 16));
+  const uint32_t prev_cap = 1u << 18;
+  int rc;
+  if ((rc = dalloc(d_rinfo, sizeof(RegionInfo))) || (rc = dalloc(d_rmark, (size_t)std::max<uint32_t>(nv, 1) * 4)) ||
+      (rc = dalloc(d_rlist, (size_t)std::max<uint32_t>(cap, 1) * 4)) || (rc = dalloc(d_rprev, (size_t)prev_cap * 4)))
+    return rc;
+  RegionInfo I;
+  std::memset(&I, 0, sizeof(I));
+  I.stale = 1;
+  I.cap = cap;
+  I.prev_cap = prev_cap;
+  I.ov_round = 64;
+  CK(cudaMemsetAsync(d_rmark.ptr, 0, (size_t)std::max<uint32_t>(nv, 1) * 4, stream));
+  CK(cudaMemcpyAsync(d_rinfo.ptr, &I, sizeof(I), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));  // `I` is stack memory
   return DSM_OK;
+}
+
+RegionDevice Engine::region_dev() {
+  RegionDevice r;
+  r.info = (RegionInfo *)d_rinfo.ptr;
+  r.mark = (uint32_t *)d_rmark.ptr;
+  r.list = (uint32_t *)d_rlist.ptr;
+  r.prev = (uint32_t *)d_rprev.ptr;
+  return r;
 }
 
 DevGraph Engine::dev_graph() {
@@ -583,6 +616,9 @@ int Engine::wait_batch(uint64_t id) {
     set_error(o.msg);
     return o.rc;
   }
+  q.unlock();
+  std::lock_guard<std::mutex> r(rmu);  // done: its results, unless released (or it failed and was reported)
+  if (results.find(id) == results.end()) return fail(DSM_ERR_NOT_FOUND, "no such batch");
   return DSM_OK;
 }
 
@@ -617,6 +653,11 @@ int Engine::prepare_filter(uint32_t id) {
     desc.pos_of_u[u] = p.enc_pos_of_u[u];
     for (uint32_t l = 0; l < 32; ++l) desc.nlc[u][l] = (uint8_t)std::min<uint32_t>(p.nlc[(size_t)u * 32 + l], 255);
   }
+  // incremental region: LDF+NLF alone reads one hop (the vertex's own
+  // adjacency), each op one more
+  uint32_t hops = filter_mode >= 2 ? (uint32_t)p.ops.size() : 0u;
+  desc.fepoch = 0xFFFFFFFFu;  // never computed: the first run is full
+  desc.full_now = 1;
   std::vector<DevFilterOp> ops(p.ops.size());
   for (size_t k = 0; k < p.ops.size(); ++k) {
     const FilterOp &o = p.ops[k];
@@ -638,7 +679,18 @@ int Engine::prepare_filter(uint32_t id) {
       d.leaf_src_count[i] = o.leaf_src_count[i];
       for (int j = 0; j < 32; ++j) d.leaf_src[i][j] = (uint16_t)o.leaf_src[i][j];
     }
+    // the merges and combines before it with the same core (validity replay)
+    for (size_t j = 0; j < k; ++j)
+      if (p.ops[j].core_u == o.core_u && p.ops[j].kind != FilterOp::kEncode) {
+        if (d.nprior == 15) {
+          hops = kRegionMaxHops + 1;  // too long a history: always full
+          break;
+        }
+        d.prior[d.nprior++] = (uint32_t)j;
+      }
   }
+  desc.hops = std::min<uint32_t>(hops, kRegionMaxHops + 1);
+  s.filter_hops = desc.hops;
   const size_t plan_bytes = sizeof(QFilterDesc) + ops.size() * sizeof(DevFilterOp);
   const uint32_t col_len = (nv + 31) / 32;
   const size_t words = std::max<uint32_t>(p.enc_words, 1);
@@ -657,7 +709,7 @@ int Engine::prepare_filter(uint32_t id) {
   return DSM_OK;
 }
 
-int Engine::launch_filter(uint32_t id, int mode) {
+int Engine::launch_filter(uint32_t id, int mode, int force_full) {
   Slot &s = slots[id];
   FilterDevice f;
   f.desc = (const QFilterDesc *)s.filter_plan.ptr;
@@ -669,8 +721,8 @@ int Engine::launch_filter(uint32_t id, int mode) {
   f.words = std::max<uint32_t>(s.plan.enc_words, 1);
   f.col_len = (nv + 31) / 32;
   f.bitmap = (uint32_t *)s.bitmap.ptr;
-  launch_query_filter(dev_graph(), f, mode, num_sms, stream);
-  stats.kernel_launches += 2 + (mode >= 2 ? f.nops : 0);
+  launch_query_filter(dev_graph(), f, mode, num_sms, stream, region_dev(), force_full || !filter_incremental);
+  stats.kernel_launches += 2 + (mode >= 2 ? 3 * f.nops : 0);
   return DSM_OK;
 }
 
@@ -703,8 +755,16 @@ int Engine::launch_filters() {
   if (filter_mode == 0) return DSM_OK;
   cudaEvent_t f0 = ev_pool[5], f1 = ev_pool[6];
   if (int r = rec(f0)) return r;
+  // the batch's region: as many hops as the farthest-reaching live query
+  uint32_t hops = 0;
+  for (uint32_t id : live_ids) hops = std::max(hops, std::min<uint32_t>(slots[id].filter_hops, kRegionMaxHops));
+  const uint32_t *hdr_n = (const uint32_t *)d_hdr.ptr;  // BatchHdr::n
+  launch_region_build(dev_graph(), region_dev(), hdr_n, (const uint4 *)d_upd.ptr, hops, num_sms, stream);
+  stats.kernel_launches += 3 + 2 * hops;
   for (uint32_t id : live_ids)
-    if (int rc = launch_filter(id, filter_mode)) return rc;
+    if (int rc = launch_filter(id, filter_mode, 0)) return rc;
+  launch_region_save(region_dev(), hdr_n, (const uint4 *)d_upd.ptr, stream);
+  ++stats.kernel_launches;
   if (int r = rec(f1)) return r;
   filter_timed = true;
   return DSM_OK;
@@ -731,7 +791,7 @@ int Engine::query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us) {
   if (qid >= slots.size() || !slots[qid].live) return fail(DSM_ERR_NOT_FOUND, "no such query");
   CK(cudaSetDevice(device));
   if (int rc = prepare_filter(qid)) return rc;
-  if (int rc = launch_filter(qid, 2)) return rc;
+  if (int rc = launch_filter(qid, 2, 1)) return rc;
   CK(cudaGetLastError());
   const Slot &s = slots[qid];
   if (bitmaps)
@@ -739,6 +799,32 @@ int Engine::query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us) {
                        stream));
   if (v_cand_us) CK(cudaMemcpyAsync(v_cand_us, s.filter_scratch.ptr, (size_t)nv * 4, cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
+  return DSM_OK;
+}
+
+// The query's resident filter state, as its last run left it: bitmaps,
+// LDF+NLF masks, and info[0] = 1 if that run recomputed every vertex,
+// info[1] = vertices it recomputed.
+int Engine::filter_state(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us, uint32_t *info) {
+  std::lock_guard<std::mutex> lk(mu);
+  if (!graph_loaded) return fail(DSM_ERR_STATE, "no graph loaded");
+  if (qid >= slots.size() || !slots[qid].live) return fail(DSM_ERR_NOT_FOUND, "no such query");
+  const Slot &s = slots[qid];
+  if (!s.bitmap.ptr || !s.filter_plan.ptr) return fail(DSM_ERR_STATE, "the query's filter has not run");
+  CK(cudaSetDevice(device));
+  if (bitmaps)
+    CK(cudaMemcpyAsync(bitmaps, s.bitmap.ptr, (size_t)s.plan.nq * ((nv + 31) / 32) * 4, cudaMemcpyDeviceToHost,
+                       stream));
+  if (v_cand_us) CK(cudaMemcpyAsync(v_cand_us, s.filter_scratch.ptr, (size_t)nv * 4, cudaMemcpyDeviceToHost, stream));
+  QFilterDesc desc;
+  RegionInfo I;
+  CK(cudaMemcpyAsync(&desc, s.filter_plan.ptr, sizeof(desc), cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(&I, d_rinfo.ptr, sizeof(I), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (info) {
+    info[0] = desc.full_now;
+    info[1] = desc.full_now ? nv : I.bound[std::min<uint32_t>(desc.hops, 63)];
+  }
   return DSM_OK;
 }
 

@@ -20,6 +20,7 @@
 #include "../../../include/dsm.h"
 #include "../host/query_plan.h"
 #include "common.cuh"
+#include "filter.cuh"
 #include "kernels.cuh"
 
 namespace dsm {
@@ -42,6 +43,7 @@ struct Slot {
   DevBuf filter_scratch;  // vcand, valid, encodings (per data vertex)
   DevBuf filter_plan;     // QFilterDesc + op list
   uint32_t filter_nops = 0;
+  uint32_t filter_hops = 0;  // hops of its incremental region (> kRegionMaxHops: always full)
   bool filter_dirty = true;  // plan or sizes must be (re)uploaded
   size_t foot = 0;           // device bytes charged to this query at admission
 };
@@ -166,6 +168,8 @@ struct Engine {
   int label_quirk = 0;
   int sort_results = 1;
   uint32_t split_min = 0, donate_depth = 0;  // donation granularity (0 = kernel default)
+  uint32_t pack_max = 1024;                  // packed last level (entries per pass; 0: off)
+  uint32_t merge_max = 64;                   // merge intersection up to this probe range (0: off)
   bool tune_next = false;                    // autotune on the next batch
   int use_graph = 0;                         // replay the batch segments as CUDA graphs
   int stall_test = 0;                        // arm matcher launches with a task nobody finishes
@@ -188,6 +192,9 @@ struct Engine {
   uint32_t nlt = 0;  // label slots in use (slot offsets per vertex: nlt + 1)
   std::vector<uint32_t> label_host;
   DevBuf d_lab, d_adj, d_cap, d_arena, d_arena_top, d_loff;
+  // incremental filter region (filter.cuh RegionInfo)
+  DevBuf d_rinfo, d_rmark, d_rlist, d_rprev;
+  int filter_incremental = 1;
 
   // queries
   std::vector<Slot> slots;
@@ -245,7 +252,10 @@ struct Engine {
   void elapsed(cudaEvent_t a, cudaEvent_t b, float *ms);
   bool capturing = false;
   int prepare_filter(uint32_t id);
-  int launch_filter(uint32_t id, int mode);
+  int launch_filter(uint32_t id, int mode, int force_full);
+  RegionDevice region_dev();
+  int region_init();
+  int filter_state(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us, uint32_t *info);
   int query_filter(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);
 
   int check_updates(const dsm_update *ups, uint32_t n);

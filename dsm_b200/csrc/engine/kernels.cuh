@@ -127,6 +127,13 @@ struct MatchArgs {
   // donated when at least donate_depth levels lie below them (1..4)
   uint32_t split_min;
   uint32_t donate_depth;
+  // packed last level (label-major runs): at most this many entries laid end
+  // to end in one pass over a chunk's candidates (0: candidates one at a time)
+  uint32_t pack_max;
+  // merge intersection: a probe range of at most this many entries is
+  // walked in tiles against the whole chunk instead of searched per entry
+  // (0: always searched)
+  uint32_t merge_max;
 };
 // Arms a matcher launch: outstanding = seeds (+ phantom, a task nothing
 // finishes: a test hook), every ring slot free for its first position.

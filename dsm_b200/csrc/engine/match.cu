@@ -20,6 +20,8 @@
 // completion brings `outstanding` to zero sets `done` and marks every
 // still-waiting ticket's slot as finished.  Every wait is bounded by a clock
 // budget that restarts whenever busy warps show progress.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace dsm {
@@ -32,6 +34,29 @@ __device__ __forceinline__ T ld_volatile(const T &x) {
 }
 
 constexpr unsigned long long kSeqDone = 1ull << 63;
+
+// One candidate of a packed last level: where its pivot range starts in the
+// concatenation (excl), its id, its own range of the last level's label
+// (run offset in 16-byte units, [a, b)), flags (bit 0: its own range is the
+// pivot; bit 1: it is an endpoint of an update of the batch).
+struct alignas(16) PackEnt {
+  uint32_t excl, cw, off, a, b, flags, pad0, pad1;
+};
+
+// Staged probe range of a packed last level (per warp, shared memory): the
+// longest last-level range in the run of a fixed position, whole when it has
+// at most kStage entries, else every 2^shift-th entry (fences); staged once
+// per level-(nq - 2) context, when first packed, if it has kStageMin entries
+// or more.  info = lane | shift << 5 | fences << 10, kStageNone: none,
+// kStageUnset: not decided yet for this context.
+constexpr uint32_t kStage = 512;
+constexpr uint32_t kStageMin = 32;
+constexpr uint32_t kStageNone = 0xFFFFFFFEu;
+constexpr uint32_t kStageUnset = 0xFFFFFFFFu;
+struct PackStage {
+  uint32_t fence[kStage];
+  uint32_t info;
+};
 
 // Lane 0 only.  Returns 1 (seed `slot`), 2 (job of ticket `slot`; the caller
 // releases the ring slot after reading it) or 0 (no more work).
@@ -107,9 +132,27 @@ __device__ void finish_task(const MatchArgs &P) {
 // kLM: label-major runs with slot offsets (the engine's graph); otherwise
 // plain id-sorted runs.  srng[L][j]: for level L and backward neighbour j,
 // the range of j's run holding the label of level L (label-major only).
+//
+// The level being scanned (the current level) keeps its iteration state in
+// warp-uniform registers (cur_*), so a chunk reads no lane's state; a level
+// with deeper levels running parks its state in lane L (lv_*) and takes it
+// back by shuffle when the search returns to it.
+//
+// Packed last level (label-major runs, P.pack_max > 0).  When a chunk of
+// level nq - 2 leaves candidates, the last level of all of them is evaluated
+// in one pass.  Candidate k's pivot range is the shortest of the last level's
+// backward ranges: those in the runs of fixed positions are the same for every
+// candidate (set up with level nq - 2), the one in the candidate's own run is
+// its own.  The pivot ranges are laid end to end (an inclusive warp scan of
+// their lengths) and scanned 32 entries at a time, each lane finding its
+// candidate by a five-step search over the scan, so short sibling ranges fill
+// whole chunks instead of one mostly idle chunk each.  When the ranges total
+// more than pack_max entries the candidates are expanded one at a time instead,
+// where long ranges can be split and donated.
 template <bool kLM>
 __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t nupd, uint32_t upd, uint32_t qo,
-                         uint32_t depth, uint32_t lo, uint32_t hi, uint32_t fval, uint2 (*srng)[16]) {
+                         uint32_t depth, uint32_t lo, uint32_t hi, uint32_t fval, uint2 (*srng)[16],
+                         PackEnt *spk, PackStage *stg) {
   const uint32_t lane = threadIdx.x & 31;
   const QDev &Q = P.qd[qo >> 8];
   const uint32_t nq = Q.nq;
@@ -130,12 +173,13 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
     my_deg = a.y;
     my_touch = P.g.lab[my_f] >> 31;
   }
-  unsigned long long alg = 0, task_cnt = 0;
+  unsigned long long alg = 0, task_cnt = 0;  // warp-uniform
 
-  // last level: the chunk's candidates are embeddings.  Listing reserves
-  // slots in the result table; a query past its listing budget reserves none
-  // (its count stays exact, the host drops its partial tuples).
-  auto emit = [&](uint32_t m, uint32_t w, uint32_t L) {
+  // The chunk's candidates m are embeddings: position L holds each lane's w,
+  // position pv (if any) each lane's cv, the others the stack.  Listing
+  // reserves slots in the result table; a query past its listing budget
+  // reserves none (its count stays exact, the host drops its partial tuples).
+  auto emit = [&](uint32_t m, uint32_t w, uint32_t L, uint32_t pv, uint32_t cv) {
     uint32_t cnt = __popc(m);
     if (cnt == 0) return;
     task_cnt += cnt;
@@ -156,7 +200,7 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
     for (uint32_t k = 0; k < nq; ++k) {
       uint32_t pk = __shfl_sync(kFull, q_pos, k);
       uint32_t fk = __shfl_sync(kFull, my_f, pk & 31);
-      if (wr) P.out_tup[s * P.W + k] = (pk == L) ? w : fk;
+      if (wr) P.out_tup[s * P.W + k] = (pk == L) ? w : (pk == pv ? cv : fk);
     }
   };
 
@@ -190,68 +234,269 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
   };
 
   if (depth >= nq) {  // a one-edge query: the seed is the embedding
-    emit(1u, 0, 0xFFFFFFFFu);
+    emit(1u, 0, 0xFFFFFFFFu, 0xFFFFFFFFu, 0);
     flush();
     return;
   }
   if (P.work_limit && publish_work()) return;  // a segment already over its limit
 
+  const uint32_t pack_max = kLM ? P.pack_max : 0u;
+  const uint32_t merge_max = kLM ? P.merge_max : 0u;
+  // the current level (warp-uniform): its pivot run, next entry, end, pending
+  // candidates of the last chunk, that chunk's first entry; its label and
+  // backward neighbours
+  uint32_t cur_base = 0, cur_pos = 0, cur_end = 0, cur_mask = 0, cur_chunk = 0, cur_pivot = 0;
+  uint32_t cur_want = 0, cur_bn = 0;
+  // level `lane`, parked while deeper levels run
+  uint32_t lv_pos = 0, lv_end = 0, lv_mask = 0, lv_chunk = 0;
+
   // Level L scans the run of its pivot: the backward neighbour with the
   // fewest candidates (label-major: entries with L's label; plain: degree).
   // [rlo, rhi) narrows the scan for a donated range (rhi = 0: all of it).
-  uint32_t lv_base = 0, lv_pos = 0, lv_end = 0, lv_mask = 0, lv_chunk = 0, lv_pivot = 0;
   auto setup_level = [&](uint32_t L, uint32_t rlo, uint32_t rhi) {
-    const uint32_t bnL = __shfl_sync(kFull, q_bn, L);
-    const bool inb = (bnL >> lane) & 1u;
+    cur_bn = __shfl_sync(kFull, q_bn, L);
+    cur_want = __shfl_sync(kFull, q_lab, L);
+    const bool inb = (cur_bn >> lane) & 1u;
     uint32_t a = 0, b = my_deg;
     if constexpr (kLM) {
-      const uint32_t want = __shfl_sync(kFull, q_lab, L);
       b = 0;
-      if (inb) {
-        if (want < P.g.nlt) {
-          const uint32_t *t = P.g.loff + (size_t)my_f * (P.g.nlt + 1) + want;
-          a = t[0];
-          b = t[1];
-        }
+      if (inb && cur_want < P.g.nlt) {
+        const uint32_t *t = P.g.loff + (size_t)my_f * (P.g.nlt + 1) + cur_want;
+        a = t[0];
+        b = t[1];
       }
-      __syncwarp();  // lanes may still read this level's previous ranges
+      // with packing, level nq - 2 also sets up the last level's ranges in
+      // the runs of the positions before it (fixed while level nq - 2 runs)
+      uint32_t fa = 0, fb = 0;
+      bool fx = false;
+      if (pack_max && L + 2 == nq) {
+        const uint32_t bnn = __shfl_sync(kFull, q_bn, L + 1);
+        const uint32_t wn = __shfl_sync(kFull, q_lab, L + 1);
+        fx = lane < L && ((bnn >> lane) & 1u);
+        if (fx && wn < P.g.nlt) {
+          const uint32_t *t = P.g.loff + (size_t)my_f * (P.g.nlt + 1) + wn;
+          fa = t[0];
+          fb = t[1];
+        }
+        alg += 8ull * __popc(bnn & ((1u << L) - 1));
+      }
+      __syncwarp();  // lanes may still read these levels' previous ranges
       if (inb) srng[L][lane] = make_uint2(a, b);
+      if (fx) srng[L + 1][lane] = make_uint2(fa, fb);
+      if (pack_max && L + 2 == nq && lane == 0) stg->info = kStageUnset;  // a new context
       __syncwarp();
-      alg += 8ull * __popc(bnL);
+      alg += 8ull * __popc(cur_bn);
     }
     const uint32_t key = inb ? ((min(b - a, 0x3FFFFFFu) << 5) | lane) : 0xFFFFFFFFu;
-    const uint32_t piv = __reduce_min_sync(kFull, key) & 31;
-    const uint32_t poff = __shfl_sync(kFull, my_off, piv);
-    const uint32_t pa = __shfl_sync(kFull, a, piv), pb = __shfl_sync(kFull, b, piv);
-    if (lane == L) {
-      lv_base = poff;
-      lv_pos = rhi ? rlo : pa;
-      lv_end = rhi ? min(rhi, pb) : pb;
-      lv_mask = 0;
-      lv_pivot = piv;
+    cur_pivot = __reduce_min_sync(kFull, key) & 31;
+    cur_base = __shfl_sync(kFull, my_off, cur_pivot);
+    const uint32_t pa = __shfl_sync(kFull, a, cur_pivot), pb = __shfl_sync(kFull, b, cur_pivot);
+    cur_pos = rhi ? rlo : pa;
+    cur_end = rhi ? min(rhi, pb) : pb;
+    cur_mask = 0;
+    cur_chunk = 0;
+  };
+
+  // The pivot of a level whose ranges are staged (label-major) or whose
+  // backward neighbours' degrees are at hand (plain): the same choice
+  // setup_level made, recomputed instead of parked.
+  auto pivot_of = [&](uint32_t L) -> uint32_t {
+    const uint32_t bnL = __shfl_sync(kFull, q_bn, L);
+    const bool inb = (bnL >> lane) & 1u;
+    uint32_t len = my_deg;
+    if constexpr (kLM) {
+      const uint2 r = inb ? srng[L][lane] : make_uint2(0, 0);
+      len = r.y - r.x;
     }
+    const uint32_t key = inb ? ((min(len, 0x3FFFFFFu) << 5) | lane) : 0xFFFFFFFFu;
+    return __reduce_min_sync(kFull, key) & 31;
+  };
+  auto pivot_base = [&](uint32_t L) -> uint32_t { return __shfl_sync(kFull, my_off, pivot_of(L)); };
+  auto resume_pivot = [&](uint32_t L) {
+    cur_pivot = pivot_of(L);
+    cur_base = __shfl_sync(kFull, my_off, cur_pivot);
+  };
+
+  uint32_t hb = 0;  // chunks since the last heartbeat
+
+  // The packed last level over the candidates m of level L = nq - 2 (lane k:
+  // candidate cw, its label word clw).  False: more than pack_max entries (or
+  // one range longer than that), nothing done.
+  auto pack_last = [&](uint32_t L, uint32_t m, uint32_t cw, uint32_t clw) -> bool {
+    const uint32_t LL = L + 1;
+    const uint32_t bnn = __shfl_sync(kFull, q_bn, LL);
+    const uint32_t wn = __shfl_sync(kFull, q_lab, LL);
+    const bool dep = (bnn >> L) & 1u;  // the last level reads the candidate's own run
+    const uint32_t fixed = bnn & ~(1u << L);
+    uint2 fr = make_uint2(0, 0);
+    uint32_t fkey = 0xFFFFFFFFu;
+    if ((fixed >> lane) & 1u) {
+      fr = srng[LL][lane];
+      fkey = (min(fr.y - fr.x, 0x3FFFFFFu) << 5) | lane;
+    }
+    const uint32_t fmin = __reduce_min_sync(kFull, fkey);
+    const uint32_t fj = fmin & 31;  // the shortest fixed range (none: fmin = ~0)
+    const uint32_t f_off = __shfl_sync(kFull, my_off, fj);
+    const uint32_t f_a = __shfl_sync(kFull, fr.x, fj);
+    const uint32_t f_b = __shfl_sync(kFull, fr.y, fj);
+    const uint32_t f_len = fmin == 0xFFFFFFFFu ? 0xFFFFFFFFu : f_b - f_a;
+    const bool cand = (m >> lane) & 1u;
+    uint32_t o_off = 0, o_a = 0, o_b = 0;
+    if (cand && dep && wn < P.g.nlt) {
+      o_off = P.g.adj[cw].x;
+      const uint32_t *t = P.g.loff + (size_t)cw * (P.g.nlt + 1) + wn;
+      o_a = t[0];
+      o_b = t[1];
+    }
+    const bool own = dep && (o_b - o_a) < f_len;
+    const uint32_t len = cand ? (own ? o_b - o_a : f_len) : 0u;
+    if (__any_sync(kFull, len > pack_max)) return false;
+    uint32_t incl = len;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFull, incl, d);
+      if (lane >= d) incl += t;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (total > pack_max) return false;
+    if (dep) alg += 8ull * __popc(m);
+    // candidate k's entry, read by the lanes whose entries fall in its range
+    __syncwarp();  // the previous pass's lanes may still read the table
+    spk[lane] = PackEnt{incl - len, cw, o_off, o_a, o_b, (own ? 1u : 0u) | ((clw >> 31) << 1), 0u, 0u};
+    uint32_t sinfo = stg->info;
+    __syncwarp();
+    if (sinfo == kStageUnset) {  // first pass of this context: stage the longest fixed range
+      const uint32_t lkey = ((fixed >> lane) & 1u) ? ((min(fr.y - fr.x, 0x3FFFFFFu) << 5) | lane) : 0u;
+      const uint32_t lmax = __reduce_max_sync(kFull, lkey);
+      const uint32_t slen = lmax >> 5, sj = lmax & 31;
+      sinfo = kStageNone;
+      if (slen >= kStageMin) {
+        uint32_t shift = 0;
+        while ((slen >> shift) > kStage) ++shift;
+        const uint32_t nf = (slen + (1u << shift) - 1) >> shift;
+        const uint32_t *src = P.g.arena + (uint64_t)__shfl_sync(kFull, my_off, sj) * 4 + __shfl_sync(kFull, fr.x, sj);
+        for (uint32_t i = lane; i < nf; i += 32) stg->fence[i] = src[(size_t)i << shift];
+        alg += 4ull * nf;
+        sinfo = sj | (shift << 5) | (nf << 10);
+      }
+      if (lane == 0) stg->info = sinfo;
+      __syncwarp();
+    }
+    const uint32_t st_j = sinfo < kStageNone ? (sinfo & 31) : 32u;
+    const uint32_t same = __ballot_sync(kFull, lane < L && q_lab == wn);
+    const bool sameP = cur_want == wn;
+    const uint32_t qvn = __shfl_sync(kFull, q_vert, LL);
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t t = base + lane;
+      bool ok = t < total;
+      // the candidate whose range holds entry t: the first lane with incl > t
+      uint32_t k = 0;
+#pragma unroll
+      for (uint32_t s = 16; s; s >>= 1) {
+        const uint32_t v = __shfl_sync(kFull, incl, k + s - 1);
+        if (v <= t) k += s;
+      }
+      const PackEnt pe = spk[k];
+      const uint32_t kx = pe.excl, kc = pe.cw, ko = pe.off, ka = pe.a, kb = pe.b, kf = pe.flags;
+      const bool kown = kf & 1u;
+      const uint64_t start = kown ? (uint64_t)ko * 4 + ka : (uint64_t)f_off * 4 + f_a;
+      const uint32_t e = ok ? P.g.arena[start + (t - kx)] : 0u;
+      const uint32_t w = e & kIdMask;
+      uint32_t lw = 0;
+      if (wn >= 31) {  // slot 31 holds every label >= 31
+        lw = ok ? P.g.lab[w] : 0u;
+        ok = ok && ((lw & kLabelMask) == wn);
+      }
+      for (uint32_t sm = same; sm; sm &= sm - 1) {
+        const uint32_t fjv = __shfl_sync(kFull, my_f, __ffs(sm) - 1);
+        ok = ok && (w != fjv);
+      }
+      if (sameP) ok = ok && (w != kc);
+      if (bitmap) ok = ok && ((bitmap[(size_t)qvn * col_len + (w >> 5)] >> (w & 31)) & 1u);
+      uint32_t probes = 0;
+      for (uint32_t bits = bnn; bits; bits &= bits - 1) {
+        const uint32_t j = __ffs(bits) - 1;
+        const uint32_t oj = __shfl_sync(kFull, my_off, j);
+        const bool piv = kown ? (j == L) : (j == fj);
+        if (ok && !piv) {
+          uint32_t ra, rb;
+          const uint32_t *lst;
+          if (j == L) {
+            lst = P.g.arena + (uint64_t)ko * 4;
+            ra = ka;
+            rb = kb;
+          } else {
+            const uint2 r = srng[LL][j];
+            lst = P.g.arena + (uint64_t)oj * 4;
+            ra = r.x;
+            rb = r.y;
+          }
+          if (j == st_j) {
+            // fences in shared memory: lo = first fence >= e; a miss there
+            // leaves the window between fences lo - 1 and lo in global memory
+            const uint32_t shift = (sinfo >> 5) & 31, nf = sinfo >> 10;
+            const uint32_t lo = lower_bound_u32(stg->fence, nf, e);
+            if (lo < nf && stg->fence[lo] == e) {
+              ok = true;
+            } else if (lo == 0 || shift == 0) {
+              ok = false;
+            } else {
+              const uint32_t wa = ra + ((lo - 1) << shift) + 1, wb = min(ra + (lo << shift), rb);
+              const uint32_t p = wa + lower_bound_u32(lst + wa, wb - wa, e);
+              ok = p < wb && lst[p] == e;
+            }
+          } else {
+            const uint32_t p = ra + lower_bound_u32(lst + ra, rb - ra, e);
+            ok = p < rb && lst[p] == e;
+          }
+          ++probes;
+        }
+      }
+      if (wn < 31) lw = ok ? P.g.lab[w] : 0u;  // touch bit of the survivors
+      if (__any_sync(kFull, ok && (lw >> 31))) {
+        for (uint32_t bits = bnn; bits; bits &= bits - 1) {
+          const uint32_t j = __ffs(bits) - 1;
+          uint32_t fjv = __shfl_sync(kFull, my_f, j), tj = __shfl_sync(kFull, my_touch, j);
+          if (j == L) {
+            fjv = kc;
+            tj = (kf >> 1) & 1u;
+          }
+          if (ok && (lw >> 31) && tj) ok = edge_live(bt, fjv, w, tp);
+        }
+      }
+      const uint32_t m2 = __ballot_sync(kFull, ok);
+      work += __popc(m2);
+      alg += 4ull * min(32u, total - base) + 4ull * __reduce_add_sync(kFull, probes);
+      emit(m2, w, LL, L, kc);
+      ++hb;
+    }
+    return true;
   };
 
   uint32_t L = depth;
   setup_level(L, lo, hi);
-  uint32_t ticks = 0;
+  uint32_t dticks = 0;  // chunks since the last donation check
   while (true) {
-    uint32_t mask = __shfl_sync(kFull, lv_mask, L);
-    if (mask == 0) {
-      uint32_t pos = __shfl_sync(kFull, lv_pos, L), end = __shfl_sync(kFull, lv_end, L);
-      if (pos >= end) {
+    if (cur_mask == 0) {
+      if (cur_pos >= cur_end) {
         if (L == depth) break;
-        --L;
+        --L;  // back to the parked level
+        cur_pos = __shfl_sync(kFull, lv_pos, L);
+        cur_end = __shfl_sync(kFull, lv_end, L);
+        cur_mask = __shfl_sync(kFull, lv_mask, L);
+        cur_chunk = __shfl_sync(kFull, lv_chunk, L);
+        cur_bn = __shfl_sync(kFull, q_bn, L);
+        cur_want = __shfl_sync(kFull, q_lab, L);
+        resume_pivot(L);
         continue;
       }
-      const uint32_t base = __shfl_sync(kFull, lv_base, L);
-      const uint32_t piv = __shfl_sync(kFull, lv_pivot, L);
-      const uint32_t *run = P.g.arena + (uint64_t)base * 4;
+      const uint32_t pos = cur_pos, end = cur_end;
+      const uint32_t *run = P.g.arena + (uint64_t)cur_base * 4;
       const uint32_t i = pos + lane;
       bool ok = i < end;
       const uint32_t e = ok ? run[i] : 0;  // entry (label-major) or id
       const uint32_t w = kLM ? (e & kIdMask) : e;
-      const uint32_t want = __shfl_sync(kFull, q_lab, L);
+      const uint32_t want = cur_want;
       uint32_t lw = 0;
       if constexpr (kLM) {
         if (want >= 31) {  // slot 31 holds every label >= 31
@@ -268,11 +513,11 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
         ok = ok && (w != fj);
       }
       if (bitmap) {
-        uint32_t qv = __shfl_sync(kFull, q_vert, L);
+        const uint32_t qv = __shfl_sync(kFull, q_vert, L);
         ok = ok && ((bitmap[(size_t)qv * col_len + (w >> 5)] >> (w & 31)) & 1u);
       }
-      const uint32_t bnL = __shfl_sync(kFull, q_bn, L);
-      uint32_t others = bnL & ~(1u << piv);
+      const uint32_t bnL = cur_bn;
+      uint32_t others = bnL & ~(1u << cur_pivot);
       uint32_t probes = 0;
       while (others) {
         uint32_t j = __ffs(others) - 1;
@@ -280,9 +525,28 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
         const uint32_t oj = __shfl_sync(kFull, my_off, j);
         if constexpr (kLM) {
           const uint2 r = srng[L][j];
-          if (ok) {
-            const uint32_t *lst = P.g.arena + (uint64_t)oj * 4;
-            const uint32_t p = r.x + lower_bound_u32(lst + r.x, r.y - r.x, e);
+          const uint32_t *lst = P.g.arena + (uint64_t)oj * 4;
+          const uint32_t nb = r.y - r.x;
+          if (nb <= merge_max) {
+            // merge: the chunk's entries (ascending across lanes) against
+            // the range in 32-entry tiles, each lane placing its entry in a
+            // tile by a five-step shuffle search; stops at the first tile
+            // that reaches the chunk's largest live entry
+            const uint32_t emax = __reduce_max_sync(kFull, ok ? e : 0u);
+            bool found = false;
+            for (uint32_t t = 0; t < nb; t += 32) {
+              const uint32_t bv = t + lane < nb ? lst[r.x + t + lane] : 0xFFFFFFFFu;
+              uint32_t k = 0;
+#pragma unroll
+              for (uint32_t sh = 16; sh; sh >>= 1)
+                if (__shfl_sync(kFull, bv, k + sh - 1) < e) k += sh;
+              found = found || (__shfl_sync(kFull, bv, k) == e && t + k < nb);
+              if (__shfl_sync(kFull, bv, 31) >= emax) break;
+            }
+            probes += ok ? 1u : 0u;
+            ok = ok && found;
+          } else if (ok) {
+            const uint32_t p = r.x + lower_bound_u32(lst + r.x, nb, e);
             ok = p < r.y && lst[p] == e;
             ++probes;
           }
@@ -308,18 +572,23 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
           if (ok && (lw >> 31) && tj) ok = edge_live(bt, fj, w, tp);
         }
       }
-      uint32_t m = __ballot_sync(kFull, ok);
+      const uint32_t m = __ballot_sync(kFull, ok);
       work += __popc(m);
       alg += (kLM ? 4ull : 8ull) * min(32u, end - pos) + 4ull * __reduce_add_sync(kFull, probes);
-      if (lane == L) {
-        lv_pos = pos + 32;
-        lv_chunk = pos;
-        lv_mask = (L == nq - 1) ? 0u : m;
+      cur_pos = pos + 32;
+      cur_chunk = pos;
+      ++hb;
+      ++dticks;
+      if (L == nq - 1) {
+        emit(m, w, L, 0xFFFFFFFFu, 0);
+      } else if (kLM && pack_max && L + 2 == nq && m) {
+        if (!pack_last(L, m, w, lw)) cur_mask = m;
+      } else {
+        cur_mask = m;
       }
-      if (L == nq - 1) emit(m, w, L);
 
-      ++ticks;
-      if ((ticks & 63) == 0) {
+      if (hb >= 64) {
+        hb = 0;
         unsigned int err = 0;
         if (lane == 0) {
           atomicAdd(&P.sc->progress.v, 1ull);
@@ -328,7 +597,8 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
         if (__shfl_sync(kFull, err, 0)) break;
         if (P.work_limit && publish_work()) break;
       }
-      if (P.donate && (ticks & 7) == 0) {
+      if (P.donate && dticks >= 8) {
+        dticks = 0;
         const uint32_t split_min = P.split_min > 64 ? P.split_min : (P.split_min ? 64u : 128u);
         const uint32_t dd = P.donate_depth ? min(P.donate_depth, 4u) : 2u;
         unsigned long long h = 0;
@@ -338,6 +608,12 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
         }
         h = __shfl_sync(kFull, h, 0);
         if (h > 0) {
+          if (lane == L) {  // park the current level, so every level reads alike
+            lv_pos = cur_pos;
+            lv_end = cur_end;
+            lv_mask = cur_mask;
+            lv_chunk = cur_chunk;
+          }
           // shallowest level with a substantial piece of work: pending
           // candidates with dd or more levels below them, or a remaining
           // range of split_min entries or more
@@ -386,7 +662,8 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
             okr = __shfl_sync(kFull, okr, 0);
             s0 = __shfl_sync(kFull, s0, 0);
             if (okr) {
-              const uint32_t pbase = __shfl_sync(kFull, lv_base, p);
+              // level p's pivot run (its ranges are still staged)
+              const uint32_t pbase = pivot_base(p);
               const uint32_t pchunk = __shfl_sync(kFull, lv_chunk, p);
               const uint32_t fsrc = __shfl_sync(kFull, my_f, (lane - 8) & 31);
               uint32_t bits = dmask;
@@ -423,6 +700,10 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
                 if (pm) lv_mask &= ~dmask;
                 else lv_end = rmid;
               }
+              if (p == L) {  // the donated piece came from the current level
+                if (pm) cur_mask &= ~dmask;
+                else cur_end = rmid;
+              }
             }
           }
         }
@@ -430,13 +711,15 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
       continue;
     }
     // descend into the lowest pending candidate of level L
-    const uint32_t b = __ffs(mask) - 1;
-    const uint32_t chunk = __shfl_sync(kFull, lv_chunk, L);
-    const uint32_t base = __shfl_sync(kFull, lv_base, L);
-    uint32_t w = P.g.arena[(uint64_t)base * 4 + chunk + b];
+    const uint32_t b = __ffs(cur_mask) - 1;
+    uint32_t w = P.g.arena[(uint64_t)cur_base * 4 + cur_chunk + b];
     if constexpr (kLM) w &= kIdMask;
+    cur_mask &= cur_mask - 1;
     if (lane == L) {
-      lv_mask = mask & (mask - 1);
+      lv_pos = cur_pos;
+      lv_end = cur_end;
+      lv_mask = cur_mask;
+      lv_chunk = cur_chunk;
       my_f = w;
       uint2 a = P.g.adj[w];
       my_off = a.x;
@@ -467,14 +750,14 @@ __global__ void k_sched_init(Sched *sc, const BatchHdr *hdr, unsigned long long 
   }
 }
 
-// Resident blocks per SM the register allocation is sized for.
-#ifndef DSM_MATCH_MIN_BLOCKS
-#define DSM_MATCH_MIN_BLOCKS 5
-#endif
-
-template <bool kLM>
-__global__ void __launch_bounds__(256, DSM_MATCH_MIN_BLOCKS) k_match(MatchArgs P) {
+// kMinBlocks: resident blocks per SM the register allocation is sized for
+// (5: 48 registers a thread; 4: 64).  Launches of 5 or more blocks per SM
+// take the first, fewer the second.
+template <bool kLM, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_match(MatchArgs P) {
   __shared__ uint2 s_rng[kLM ? 8 : 1][16][16];
+  __shared__ PackEnt s_pack[kLM ? 8 : 1][32];
+  __shared__ PackStage s_stage[kLM ? 8 : 1];
   const uint32_t lane = threadIdx.x & 31;
   if (*P.abort_flag & kErrArena) return;  // the batch was refused before its insert
   const uint32_t nupd = P.hdr->n;
@@ -509,7 +792,8 @@ __global__ void __launch_bounds__(256, DSM_MATCH_MIN_BLOCKS) k_match(MatchArgs P
       hi = __shfl_sync(kFull, word, 4);
       fval = __shfl_sync(kFull, word, (lane + 8) & 31);
     }
-    run_task<kLM>(P, bt, nupd, upd, qo, depth, lo, hi, fval, s_rng[kLM ? (threadIdx.x >> 5) : 0]);
+    run_task<kLM>(P, bt, nupd, upd, qo, depth, lo, hi, fval, s_rng[kLM ? (threadIdx.x >> 5) : 0],
+                  s_pack[kLM ? (threadIdx.x >> 5) : 0], &s_stage[kLM ? (threadIdx.x >> 5) : 0]);
     finish_task(P);
   }
 }
@@ -522,14 +806,19 @@ void launch_sched_init(Sched *sc, const BatchHdr *hdr, unsigned long long *job_s
 }
 
 void launch_match(const MatchArgs &a, int blocks, cudaStream_t s) {
-  if (a.g.loff) k_match<true><<<blocks, 256, 0, s>>>(a);
-  else k_match<false><<<blocks, 256, 0, s>>>(a);
+  int dev = 0, sms = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const bool wide = blocks < 5 * std::max(sms, 1);  // fewer than 5 blocks per SM: 64 registers
+  if (!a.g.loff) k_match<false, 5><<<blocks, 256, 0, s>>>(a);
+  else if (wide) k_match<true, 4><<<blocks, 256, 0, s>>>(a);
+  else k_match<true, 5><<<blocks, 256, 0, s>>>(a);
 }
 
 int match_max_blocks_per_sm() {
   int n = 0, m = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_match<true>, 256, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_match<false>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_match<true, 5>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_match<false, 5>, 256, 0);
   return n < m ? n : m;
 }
 

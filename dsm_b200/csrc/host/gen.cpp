@@ -57,15 +57,29 @@ uint32_t sample_cdf(const std::vector<double> &cdf, Rng &r) {
 }
 
 // Distinct undirected edges without self loops until `m` are found, then a
-// seeded shuffle fixes their order.  Each round draws in fixed chunks of 2^20
-// edges, chunk c with its own generator seeded from the round's seed and c,
-// so the chunks run on all host threads and the result does not depend on
-// the thread count.
+// seeded shuffle fixes their order.  Graphs of up to 2^25 edges draw from
+// the one generator in sequence.  Larger ones draw each round in fixed chunks
+// of 2^20 edges, chunk c with its own generator seeded from the round's seed
+// and c, so the chunks run on all host threads and the result does not
+// depend on the thread count.
 template <class Draw>
 std::vector<uint64_t> distinct_edges(uint64_t m, Rng &r, Draw draw) {
   std::vector<uint64_t> keys;
   keys.reserve(m + m / 4);
   constexpr size_t kGrain = 1u << 20;
+  if (m <= (1ull << 25)) {
+    while (keys.size() < m) {
+      const uint64_t need = m - keys.size();
+      const uint64_t batch = need + need / 8 + 1024;
+      for (uint64_t k = 0; k < batch; ++k) {
+        uint32_t a, b;
+        draw(r, a, b);
+        if (a != b) keys.push_back(edge_key(a, b));
+      }
+      parallel_sort(keys);
+      keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    }
+  }
   while (keys.size() < m) {
     const uint64_t need = m - keys.size();
     const uint64_t batch = need + need / 8 + 1024;

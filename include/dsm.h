@@ -75,10 +75,13 @@ const char *dsm_last_error(dsm_engine *e);
 #define DSM_OPT_DONATE_DEPTH 12 /* work donation: hand out pending candidates with at least
                                    this many levels below them (0 = default 2; 1..4) */
 #define DSM_OPT_AUTOTUNE 13     /* 1: the next batch times its matcher launch under each
-                                   candidate setting (resident blocks per SM x split
-                                   threshold x donation depth) on its own union graph and
-                                   keeps the fastest in DSM_OPT_WARPS_PER_SM /
-                                   DSM_OPT_SPLIT_MIN / DSM_OPT_DONATE_DEPTH; its results
+                                   candidate setting on its own union graph -- first the
+                                   intersection tile (DSM_OPT_PACK_MAX in {0, 256, 1024,
+                                   4096} x DSM_OPT_MERGE_MAX in {0, 64, 256}), then resident
+                                   blocks per SM x split threshold x donation depth -- and
+                                   keeps the fastest in DSM_OPT_PACK_MAX / DSM_OPT_MERGE_MAX /
+                                   DSM_OPT_WARPS_PER_SM / DSM_OPT_SPLIT_MIN /
+                                   DSM_OPT_DONATE_DEPTH; its results
                                    are those of any setting.  Reads 1 until that batch ran. */
 #define DSM_OPT_GRAPH 14        /* 1: each batch's two device segments (uploads .. matcher, and
                                    deletes .. downloads) are captured into CUDA graphs and
@@ -109,6 +112,23 @@ const char *dsm_last_error(dsm_engine *e);
                                    count) and it lists no tuples.  Every other count stays
                                    exact.  (With DSM_OPT_FILTER > 0 the filter prunes
                                    partial embeddings, so fewer reach the bound.) */
+#define DSM_OPT_FILTER_INCREMENTAL 20 /* 1 (default): a batch's filter recomputes only the
+                                   data vertices within (the query's op count) hops of
+                                   the endpoints of its own and the previous batch's
+                                   updates, falling back to every vertex when that region
+                                   is large or the query's state is not the previous
+                                   batch's; 0: every vertex, every batch.  Same bitmaps. */
+#define DSM_OPT_MERGE_MAX 21     /* matcher set intersection: a backward neighbour's label range
+                                   of at most this many entries is intersected with a whole
+                                   32-entry chunk by a ballot/shuffle merge over 32-entry tiles
+                                   instead of a binary search per entry (default 64; 0: always
+                                   searched; at most 2^16).  Results do not depend on it. */
+#define DSM_OPT_PACK_MAX 19     /* matcher intersection tile: the candidates one 32-entry
+                                   chunk leaves at the second-to-last query vertex have
+                                   their last-level ranges laid end to end and scanned
+                                   together when they total at most this many entries
+                                   (default 1024; 0: each candidate scanned on its own;
+                                   at most 2^20).  Results do not depend on it. */
 int dsm_engine_set_option(dsm_engine *e, int option, int64_t value);
 int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value);
 
@@ -157,6 +177,14 @@ int dsm_query_order(dsm_engine *e, uint32_t qid, uint32_t u, uint32_t v, uint32_
  * clusterFilter + compact (filter.cuh:119-137).  v_cand_us (nv words, may be
  * NULL): bit u set when v passes LDF+NLF for u (d_v_candidate_us_). */
 int dsm_query_filter(dsm_engine *e, uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us);
+/* The filter state the last batch left for query qid (DSM_OPT_FILTER > 0),
+ * without recomputing it: the bitmaps and v_cand_us as dsm_query_filter
+ * gives them, for that batch's union graph.  info (2 words, may be NULL):
+ * info[0] = 1 if that run recomputed every data vertex, 0 if it recomputed
+ * only the incremental region; info[1] = data vertices it recomputed.  No
+ * reference counterpart: the reference recomputes the whole filter every
+ * batch (main.cu:213, filter.cu:1525-1654). */
+int dsm_query_filter_state(dsm_engine *e, uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us, uint32_t *info);
 
 /* Host only (no engine, no GPU): the plan the engine would build for a
  * query.  orders / bn_masks: one row of nq words per ordered query edge, in

@@ -1153,7 +1153,8 @@ int orc_stream_apply(orc_stream *h, uint32_t n, const uint32_t *ups, int list) {
   if (S.complete < n && list) {
     // drop tuples of updates past the complete prefix
     uint64_t keep = 0;
-    for (uint32_t i = 0; i < S.complete; ++i) keep += S.count[i];
+    for (uint32_t i = 0; i < S.complete; ++i)
+      if (!(S.count[i] & kIncomplete)) keep += S.count[i];  // over the work limit: nothing listed
     S.tuples.resize(keep * S.nq);
   }
   for (uint32_t i = S.complete; i < n; ++i) S.count[i] = 0;

@@ -194,8 +194,9 @@ class Stream:
         flat = _arr(ptr, tot.value * self.nq).reshape(-1, self.nq)
         out, pos = [], 0
         for c in counts:
-            out.append(flat[pos:pos + int(c)])
-            pos += int(c)
+            k = 0 if int(c) >> 63 else int(c)  # a search over the work limit lists nothing
+            out.append(flat[pos:pos + k])
+            pos += k
         return signs, counts, out
 
     def apply_graph(self, updates):

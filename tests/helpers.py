@@ -6,9 +6,44 @@ budget per slice of updates: it applies every update to its graph, but
 enumerates only while the slice's budget lasts (`Stream.complete` updates
 have results).  The engine always runs whole batches; the comparison covers
 every update the oracle could afford, and the graphs are compared in full."""
+import functools
+
 import numpy as np
 
 from oracle import oracle as orc
+
+
+@functools.lru_cache(maxsize=None)
+def _generated(config, seed, scale_log2, num_batches):
+    import dsm_b200 as d
+    return d.Workload(config, seed=seed, scale_log2=scale_log2, num_batches=num_batches)
+
+
+class _FirstBatches:
+    """The first `nb` batches of a generated workload (the update stream is
+    generated in order, so it equals a workload generated with nb batches)."""
+
+    def __init__(self, w, nb):
+        self._w = w
+        self.nv, self.labels, self.edges, self.queries = w.nv, w.labels, w.edges, w.queries
+        self.batch_sizes = w.batch_sizes[:nb]
+        self.updates = w.updates[:int(self.batch_sizes.sum())]
+
+    def batches(self):
+        pos = 0
+        for s in self.batch_sizes:
+            yield self.updates[pos:pos + int(s)]
+            pos += int(s)
+
+
+def workload(config, seed=0, scale_log2=0, num_batches=0):
+    """A seeded workload, generated once per test session (generation screens
+    query candidates on the host and takes seconds to minutes; the tests only
+    read it)."""
+    if num_batches == 0:
+        return _generated(config, seed, scale_log2, 0)
+    return _FirstBatches(_generated(config, seed, scale_log2, max(num_batches, 3)), num_batches)
+
 
 BYTES_PER_EMBEDDING = 64  # work budget per embedding the oracle is allowed
 

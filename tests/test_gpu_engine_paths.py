@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import dsm_b200 as d
-from tests.helpers import compare_batch, oracle_apply, oracle_stream, run_stream
+from tests.helpers import compare_batch, oracle_apply, oracle_stream, run_stream, workload
 
 pytestmark = pytest.mark.gpu
 OOM = 2
@@ -30,7 +30,7 @@ def _same(ra, rb):
 def test_plain_form_equals_batched():
     """32 config-3 queries (scaled graph): one launch per query per batch
     gives the batched form's listed results, update by update."""
-    w = d.Workload(3, scale_log2=-6, num_batches=2)
+    w = workload(3, scale_log2=-6, num_batches=2)
     bs = [b[:512] for b in w.batches()]
     qs = w.queries[:32]
     a, _ = _fresh(w.nv, w.labels, w.edges, qs)
@@ -53,17 +53,20 @@ def test_query_list_limit_drops_only_heavy_queries(plain):
     """With a per-query listing budget, a query that would list more in a
     batch reports exact counts and no tuples; every other query is listed
     exactly as without the budget."""
-    w = d.Workload(3, scale_log2=-6, num_batches=1)
-    b = next(w.batches())[:512]
+    w = workload(3, scale_log2=-6, num_batches=1)
+    b = next(w.batches())[:256]
     qs = w.queries[:16]
-    full, _ = _fresh(w.nv, w.labels, w.edges, qs)
+    # the unbudgeted run must list everything (no batch-wide downgrade)
+    full, _ = _fresh(w.nv, w.labels, w.edges, qs, OPT_LIST_LIMIT=1 << 33)
     rf = full.run_batch(b)
+    assert rf.listed
     per_q = rf.counts.sum(axis=1)
     nz = np.sort(per_q[per_q > 0])
     assert len(nz) >= 2
     limit = int(nz[len(nz) // 2])  # about half of the non-empty queries go over
-    lim, _ = _fresh(w.nv, w.labels, w.edges, qs, OPT_QUERY_LIST_LIMIT=limit, OPT_PLAIN=plain)
+    lim, _ = _fresh(w.nv, w.labels, w.edges, qs, OPT_QUERY_LIST_LIMIT=limit, OPT_PLAIN=plain, OPT_LIST_LIMIT=1 << 33)
     rl = lim.run_batch(b)
+    assert rl.listed
     assert np.array_equal(rf.counts, rl.counts)
     want = per_q <= limit
     assert np.array_equal(rl.query_listed, want)
@@ -80,7 +83,7 @@ def test_query_list_limit_drops_only_heavy_queries(plain):
 
 
 def test_graph_apply_equals_oracle_and_matching_continues():
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -112,7 +115,7 @@ def test_arena_compaction_long_insert_stream():
     """A config-1 graph takes 16 batches of 4096 mostly-insert updates (its
     edge count grows 3x): runs relocate, the arena compacts, and every batch
     and the final graph equal the oracle."""
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -130,7 +133,7 @@ def test_arena_refusal_leaves_graph_unchanged():
     relocations do not fit the arena is refused before it writes anything
     (DSM_ERR_OOM, graph unchanged); with room it then runs and equals the
     oracle."""
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q], OPT_LIST=0)  # counts: no result table to regrow
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -166,7 +169,7 @@ def test_work_limit_flags_equal_oracle(form):
     bound as in the oracle (whatever the launch form and scheduling), every
     other count and tuple list is exact, and flagged ones list nothing."""
     lim = 20_000
-    w = d.Workload(3, scale_log2=-6, num_batches=1)
+    w = workload(3, scale_log2=-6, num_batches=1)
     b = next(w.batches())[:512]
     qs = w.queries[:12]
     opts = {"OPT_WORK_LIMIT": lim}
@@ -198,3 +201,50 @@ def test_work_limit_flags_equal_oracle(form):
     assert flagged > 0  # the bound was reached somewhere
     assert e.stats()["over_limit"] >= flagged
     e.close()
+
+
+def _same_flagged(ra, rb):
+    """Equal results where counts are exact; the same (query, update) pairs
+    flagged over the work limit (their partial counts depend on scheduling)."""
+    assert np.array_equal(ra.signs, rb.signs)
+    fa, fb = (ra.counts & d.INCOMPLETE) != 0, (rb.counts & d.INCOMPLETE) != 0
+    assert np.array_equal(fa, fb)
+    assert np.array_equal(ra.counts[~fa], rb.counts[~fb])
+    assert np.array_equal(ra.offsets, rb.offsets)
+    assert np.array_equal(ra.tuples, rb.tuples)
+
+
+@pytest.mark.parametrize("cfg,scale,nqs", [(2, -6, 3), (3, -6, 64), (4, -8, 16), (5, -4, 8)])
+def test_intersection_tile_settings_agree(cfg, scale, nqs):
+    """DSM_OPT_PACK_MAX (the packed last level) and DSM_OPT_MERGE_MAX (merge
+    intersection): both off, a tile small enough that most passes fall back
+    to one candidate at a time, the defaults, and the largest all give the
+    same listed results and work-limit flags, and the first query's equal the
+    oracle's (same limit)."""
+    lim = 200_000
+    w = workload(cfg, scale_log2=scale, num_batches=1)
+    b = next(w.batches())[:1024]
+    qs = w.queries[:nqs]
+    res = []
+    for pk, mg in ((0, 0), (32, 256), (1024, 64), (1 << 20, 1 << 16)):
+        e, qids = _fresh(w.nv, w.labels, w.edges, qs, OPT_PACK_MAX=pk, OPT_MERGE_MAX=mg, OPT_WORK_LIMIT=lim)
+        assert e.get_option(d.OPT_PACK_MAX) == pk and e.get_option(d.OPT_MERGE_MAX) == mg
+        res.append(e.run_batch(b))
+        e.close()
+    for r in res[1:]:
+        _same_flagged(res[0], r)
+    st = oracle_stream(w.nv, w.labels, w.edges, qs[0])
+    st.set_work_limit(lim)
+    s, c, t = st.apply(b, listed=True)
+    r = res[2]
+    got = r.counts[r.query_index(qids[0])]
+    fo, fe = (c & d.INCOMPLETE) != 0, (got & d.INCOMPLETE) != 0
+    assert np.array_equal(fo, fe)
+    assert np.array_equal(got[~fe], c[~fo])
+    for i in range(len(b)):
+        assert np.array_equal(r.tuples_of(qids[0], i), t[i] if not fo[i] else t[i][:0]), f"update {i}"
+    exact = res[0].counts[(res[0].counts & d.INCOMPLETE) == 0]
+    flagged = int(((res[0].counts & d.INCOMPLETE) != 0).sum())
+    # config 5's twelve-vertex cyclic queries match rarely: there the
+    # bounded (flagged) searches are what the settings must agree on
+    assert int(exact.astype(np.float64).sum()) > (1000 if cfg != 5 else 0) or (cfg == 5 and flagged > 0)

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import dsm_b200 as d
-from tests.helpers import compare_batch, oracle_apply, oracle_stream
+from tests.helpers import compare_batch, oracle_apply, oracle_stream, workload
 
 pytestmark = pytest.mark.gpu
 
@@ -23,7 +23,7 @@ NOT_FOUND = 9
 
 
 def _setup(graph=0):
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     e = d.Engine(0)
     e.set_option(d.OPT_GRAPH, graph)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 import dsm_b200 as d
-from tests.helpers import compare_batch, oracle_apply, oracle_stream, run_stream
+from tests.helpers import compare_batch, oracle_apply, oracle_stream, run_stream, workload
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -46,7 +46,7 @@ def test_c1_stream_one_update_per_batch():
     """Config 1: R-MAT 4096 vertices, one 5-vertex one-cycle query, 4276
     single-update batches (3276 re-inserts, 1000 deletes), graph checked
     every 500 batches and at the end."""
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -61,7 +61,7 @@ def test_c1_stream_one_update_per_batch():
 def test_c1_as_large_batches():
     """The same stream cut into batches of 512: sequential semantics inside a
     batch must give the same per-update sets as one update per batch."""
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -76,7 +76,7 @@ def test_c2_scaled_counts(qi):
     queries) at 2^14 vertices, two batches of 4096 mixed updates, count mode:
     exact per-update counts wherever the oracle's budget reaches, and the
     whole graph after every batch."""
-    w = d.Workload(2, scale_log2=-6, num_batches=2)
+    w = workload(2, scale_log2=-6, num_batches=2)
     q = w.queries[qi]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q], OPT_LIST=0)
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -90,7 +90,7 @@ def test_c2_scaled_counts(qi):
 def test_c2_scaled_listing(qi):
     """Same workload, listed: every affordable update's sorted embedding set
     in the first batch of 4096."""
-    w = d.Workload(2, scale_log2=-6, num_batches=1)
+    w = workload(2, scale_log2=-6, num_batches=1)
     q = w.queries[qi]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -104,7 +104,7 @@ def test_c4_thirty_two_labels(k):
     """Config 4 shape (R-MAT, 32 uniform labels: the last label slot is in
     use) at 2^16 vertices; the first two pool queries that carry label 31.
     Listed, two lognormal-size batches."""
-    w = d.Workload(4, scale_log2=-8, num_batches=2)
+    w = workload(4, scale_log2=-8, num_batches=2)
     q = [q for q in w.queries if 31 in q.labels.tolist()][k]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q])
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -145,7 +145,7 @@ def test_autotuned_batch_equals_oracle():
     """DSM_OPT_AUTOTUNE: the first batch times every candidate launch setting
     on its own union graph and keeps the fastest; its results and the next
     batch's (run with the tuned setting) equal the oracle's."""
-    w = d.Workload(2, scale_log2=-6, num_batches=2)
+    w = workload(2, scale_log2=-6, num_batches=2)
     q = w.queries[2]
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [q], OPT_LIST=0, OPT_AUTOTUNE=1)
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -165,7 +165,7 @@ def test_graph_replay_equals_eager():
     """DSM_OPT_GRAPH: the batch segments run as CUDA graphs (captured, then
     updated in place while their topology repeats); listed results and the
     graph equal the eager engine's, batch by batch."""
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     eager, (qa,) = _fresh(w.nv, w.labels, w.edges, [q])
     graph, (qb,) = _fresh(w.nv, w.labels, w.edges, [q], OPT_GRAPH=1)
@@ -190,7 +190,7 @@ def test_graph_replay_equals_eager():
 def test_graph_replay_varying_sizes():
     """Batches of very different sizes replay the same two executable graphs:
     the kernels read the sizes from the device header."""
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     eager, (qa,) = _fresh(w.nv, w.labels, w.edges, [q])
     graph, (qb,) = _fresh(w.nv, w.labels, w.edges, [q], OPT_GRAPH=1)
@@ -214,7 +214,7 @@ def test_graph_replay_varying_sizes():
 def test_graph_replay_with_filter_multi_query():
     """Graph replay with the cluster filter inside the captured segment, 16
     config-3 queries, against the oracle."""
-    w = d.Workload(3, scale_log2=-6, num_batches=2)
+    w = workload(3, scale_log2=-6, num_batches=2)
     bs = [b[:512] for b in w.batches()]
     qs = w.queries[:16]
     e, qids = _fresh(w.nv, w.labels, w.edges, qs, OPT_GRAPH=1, OPT_FILTER=2)
@@ -226,7 +226,7 @@ def test_graph_replay_with_filter_multi_query():
 
 
 def test_listing_limit_downgrades_to_counts():
-    w = d.Workload(1, scale_log2=-2)
+    w = workload(1, scale_log2=-2)
     b = np.concatenate(list(w.batches())[:400])
     e, (qid,) = _fresh(w.nv, w.labels, w.edges, [w.queries[0]], OPT_LIST_LIMIT=64)
     r = e.run_batch(b)
@@ -241,7 +241,7 @@ def test_listing_limit_downgrades_to_counts():
 def test_multi_query_batched():
     """Config 3 shape scaled: 32 queries of 4-12 vertices in one launch; each
     query's listed results equal the oracle's for that query alone."""
-    w = d.Workload(3, scale_log2=-6, num_batches=2)
+    w = workload(3, scale_log2=-6, num_batches=2)
     bs = [b[:1024] for b in w.batches()]
     qs = w.queries[:32]
     e, qids = _fresh(w.nv, w.labels, w.edges, qs)
@@ -253,7 +253,7 @@ def test_multi_query_batched():
 
 def test_multi_query_counts_all_256():
     """All 256 config-3 queries (scaled graph) in one launch, count mode."""
-    w = d.Workload(3, scale_log2=-6, num_batches=1)
+    w = workload(3, scale_log2=-6, num_batches=1)
     b = next(w.batches())[:256]
     e, qids = _fresh(w.nv, w.labels, w.edges, w.queries, OPT_LIST=0)
     assert len(qids) == 256
@@ -298,7 +298,7 @@ def test_batch_edge_cases():
 
 
 def test_one_edge_query_and_count_mode():
-    w = d.Workload(1, scale_log2=-2)
+    w = workload(1, scale_log2=-2)
     q = d.Query.from_edges([0, 1], [(0, 1)])
     big = np.concatenate(list(w.batches())[:300])
     e, (qid, _) = _fresh(w.nv, w.labels, w.edges, [q, w.queries[0]])
@@ -318,7 +318,7 @@ def test_one_edge_query_and_count_mode():
 def test_result_regrow_and_no_donation_agree():
     """A tiny result capacity forces the overflow-and-rerun path; donation
     off gives the same sets."""
-    w = d.Workload(2, scale_log2=-6, num_batches=1)
+    w = workload(2, scale_log2=-6, num_batches=1)
     q = w.queries[2]
     b = next(w.batches())[:1024]
     st = oracle_stream(w.nv, w.labels, w.edges, q)
@@ -329,7 +329,7 @@ def test_result_regrow_and_no_donation_agree():
 
 
 def test_retire_and_register_between_batches():
-    w = d.Workload(3, scale_log2=-6, num_batches=3)
+    w = workload(3, scale_log2=-6, num_batches=3)
     bs = [b[:512] for b in w.batches()]
     qs = w.queries[:6]
     e, qids = _fresh(w.nv, w.labels, w.edges, qs[:4])

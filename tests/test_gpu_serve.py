@@ -10,13 +10,13 @@ import numpy as np
 import pytest
 
 import dsm_b200 as d
-from tests.helpers import compare_batch, oracle_apply, oracle_stream
+from tests.helpers import compare_batch, oracle_apply, oracle_stream, workload
 
 pytestmark = pytest.mark.gpu
 
 
 def test_merged_batches_equal_oracle():
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     e = d.Engine(0)
     e.load_graph_edges(w.nv, w.labels, w.edges)
@@ -43,7 +43,7 @@ def test_merged_batches_equal_oracle():
 
 
 def test_alone_equals_mix_with_churn():
-    w = d.Workload(3, scale_log2=-6, num_batches=2)
+    w = workload(3, scale_log2=-6, num_batches=2)
     ups = np.concatenate([b[:512] for b in w.batches()])
     chunks = [ups[i:i + 128] for i in range(0, len(ups), 128)]
     qs = w.queries[:16]
@@ -89,7 +89,7 @@ def test_alone_equals_mix_with_churn():
 
 
 def test_admission_waits_for_memory():
-    w = d.Workload(1)
+    w = workload(1)
     q = w.queries[0]
     e = d.Engine(0)
     e.load_graph_edges(w.nv, w.labels, w.edges)
@@ -127,7 +127,7 @@ def test_admission_waits_for_memory():
 
 
 def test_serving_errors_and_restart():
-    w = d.Workload(1)
+    w = workload(1)
     e = d.Engine(0)
     e.load_graph_edges(w.nv, w.labels, w.edges)
     qid = e.register(w.queries[0])
@@ -149,7 +149,7 @@ def test_snapshot_resume(tmp_path):
     """An engine resumed from a snapshot (graph, queries with their ids, batch
     counter) gives the same results for the rest of the stream as the engine
     that wrote it."""
-    w = d.Workload(1)
+    w = workload(1)
     ups = w.updates
     half = len(ups) // 2
     a = d.Engine(0)
