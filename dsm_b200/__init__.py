@@ -20,7 +20,7 @@ ERR = {1: "PARSE", 2: "OOM", 3: "OVERFLOW", 4: "TIMEOUT", 5: "LIMIT", 6: "ARG", 
 
 OPT_LIST, OPT_FILTER, OPT_RESULT_CAP, OPT_WARPS_PER_SM, OPT_DONATE, OPT_TIMEOUT_MS, OPT_LABEL_QUIRK, OPT_SORT, \
     OPT_LIST_LIMIT, OPT_MEM_BUDGET, OPT_SPLIT_MIN, OPT_DONATE_DEPTH, OPT_AUTOTUNE, OPT_GRAPH, OPT_STALL_TEST, \
-    OPT_PLAIN, OPT_QUERY_LIST_LIMIT, OPT_WORK_LIMIT, OPT_PACK_MAX, OPT_FILTER_INCREMENTAL, OPT_MERGE_MAX = range(1, 22)
+    OPT_PLAIN, OPT_QUERY_LIST_LIMIT, OPT_WORK_LIMIT, OPT_PACK_MAX, OPT_FILTER_INCREMENTAL, OPT_MERGE_MAX, OPT_BFS_LEVELS, OPT_BFS_ROWS = range(1, 24)
 INCOMPLETE = np.uint64(1 << 63)  # bit of a count whose search went over DSM_OPT_WORK_LIMIT
 
 if not os.path.exists(LIB_PATH):

@@ -95,6 +95,14 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
       E.donate_depth = (uint32_t)value;
       return DSM_OK;
     case DSM_OPT_FILTER_INCREMENTAL: E.filter_incremental = value ? 1 : 0; return DSM_OK;
+    case DSM_OPT_BFS_LEVELS:
+      if (value < 0 || value > 8) return E.fail(DSM_ERR_ARG, "breadth-first levels 0..8");
+      E.bfs_levels = (uint32_t)value;
+      return DSM_OK;
+    case DSM_OPT_BFS_ROWS:
+      if (value < 32 || value > (1ll << 28)) return E.fail(DSM_ERR_ARG, "row table 32..2^28 rows");
+      E.bfs_rows = (uint64_t)value;
+      return DSM_OK;
     case DSM_OPT_MERGE_MAX:
       if (value < 0 || value > (1 << 16)) return E.fail(DSM_ERR_ARG, "merge threshold 0..2^16 entries");
       E.merge_max = (uint32_t)value;
@@ -145,6 +153,8 @@ int dsm_engine_get_option(dsm_engine *e, int option, int64_t *value) {
     case DSM_OPT_PACK_MAX: *value = E.pack_max; return DSM_OK;
     case DSM_OPT_FILTER_INCREMENTAL: *value = E.filter_incremental; return DSM_OK;
     case DSM_OPT_MERGE_MAX: *value = E.merge_max; return DSM_OK;
+    case DSM_OPT_BFS_LEVELS: *value = E.bfs_levels; return DSM_OK;
+    case DSM_OPT_BFS_ROWS: *value = (int64_t)E.bfs_rows; return DSM_OK;
     case DSM_OPT_AUTOTUNE: *value = E.tune_next ? 1 : 0; return DSM_OK;
     case DSM_OPT_GRAPH: *value = E.use_graph; return DSM_OK;
     case DSM_OPT_STALL_TEST: *value = E.stall_test; return DSM_OK;

@@ -157,6 +157,8 @@ int Engine::launch_front(Staged &S) {
   S.work_limit = S.match ? work_limit : 0;
   if (S.work_limit && (rc = dalloc(d_segwork, S.nseg * 8))) return rc;
   if (S.match && (rc = dalloc(d_seeds, S.seed_cap * 16))) return rc;
+  if (S.match && (bfs_levels || (tune_next && !S.plain)) && (rc = dalloc(d_rows, bfs_rows * sizeof(JobRec))))
+    return rc;
   if (!d_jobs.ptr) {
     if ((rc = dalloc(d_jobs, (size_t)job_ring * sizeof(JobRec))) || (rc = dalloc(d_job_seq, (size_t)job_ring * 8)))
       return rc;
@@ -271,6 +273,9 @@ int Engine::launch_front(Staged &S) {
     key_append(key, query_gen);
     key_append(key, filter_mode);
     key_append(key, filter_incremental);
+    key_append(key, bfs_levels);
+    key_append(key, d_rows.ptr);
+    key_append(key, d_rows.bytes);
     key_append(key, stall_test);
     key_append(key, h_sched.ptr);
     key_append(key, h_qlisted.ptr);
@@ -278,8 +283,7 @@ int Engine::launch_front(Staged &S) {
       if (int r = seg_a_kernels(S, ca, es, au, sa, true)) return r;
       if (S.match) {
         if (int r = rec(ev_pool[2])) return r;
-        launch_match(ma, blocks, stream);
-        ++stats.kernel_launches;
+        if (int r = launch_match_seq(ma, blocks, bfs_levels)) return r;
         if (int r = rec(ev_pool[3])) return r;
       }
       return read_back();
@@ -301,6 +305,37 @@ int Engine::launch_front(Staged &S) {
   return DSM_OK;
 }
 
+// The matcher launch of a batch.  With breadth-first levels (label-major
+// runs only) it is two launches: the first writes every prefix of 2 +
+// `levels` positions to the row table instead of descending (while the
+// table has room; beyond it, tasks go on depth-first), the second takes
+// those rows as its tasks -- the reference's breadth-first expansion before
+// its depth-first matcher (gpu_match.cu:1291-1357) and its row-by-row edge
+// join (join.cu:106-221), in place of one launch per level.
+int Engine::launch_match_seq(const MatchArgs &ma, int blocks, uint32_t levels) {
+  if (levels == 0 || !ma.g.loff || !d_rows.ptr) {
+    launch_match(ma, blocks, stream);
+    ++stats.kernel_launches;
+    return DSM_OK;
+  }
+  const unsigned long long cap = d_rows.bytes / sizeof(JobRec);
+  unsigned long long *cnt = (unsigned long long *)((char *)d_misc.ptr + 160);
+  CK(cudaMemsetAsync(cnt, 0, 8, stream));
+  MatchArgs a1 = ma;
+  a1.bfs_stop = 2 + levels;
+  a1.rows_out = (JobRec *)d_rows.ptr;
+  a1.rows_cnt = cnt;
+  a1.rows_cap = cap;
+  launch_match(a1, blocks, stream);
+  launch_rows_arm((Sched *)d_sched.ptr, cnt, cap, stream);
+  launch_sched_init((Sched *)d_sched.ptr, nullptr, (unsigned long long *)d_job_seq.ptr, job_ring, stream, stall_test);
+  MatchArgs a2 = ma;
+  a2.rows_in = (const JobRec *)d_rows.ptr;
+  launch_match(a2, blocks, stream);
+  stats.kernel_launches += 4;
+  return DSM_OK;
+}
+
 // The matcher, eagerly: one launch for every query, or (plain form) one launch
 // per query with a host round trip after each; the scheduler state of all of
 // them is combined into h_sched.
@@ -308,8 +343,7 @@ int Engine::match_eager(Staged &S, MatchArgs &ma, SeedArgs &sa, int blocks) {
   const int sblocks = num_sms * 4;
   if (!S.plain) {
     if (int r = rec(ev_pool[2])) return r;
-    launch_match(ma, blocks, stream);
-    ++stats.kernel_launches;
+    if (int r = launch_match_seq(ma, blocks, bfs_levels)) return r;
     if (int r = rec(ev_pool[3])) return r;
     CK(cudaMemcpyAsync(h_sched.ptr, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
     CK(cudaMemcpyAsync((char *)h_sched.ptr + sizeof(Sched), d_misc.ptr, 64, cudaMemcpyDeviceToHost, stream));
@@ -332,8 +366,8 @@ int Engine::match_eager(Staged &S, MatchArgs &ma, SeedArgs &sa, int blocks) {
     launch_seeds(sa, sblocks, stream);
     launch_sched_init((Sched *)d_sched.ptr, (const BatchHdr *)d_hdr.ptr, (unsigned long long *)d_job_seq.ptr,
                       job_ring, stream, stall_test);
-    launch_match(ma, blocks, stream);
-    stats.kernel_launches += 3;
+    stats.kernel_launches += 2;
+    if (int r = launch_match_seq(ma, blocks, bfs_levels)) return r;
     CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     total.nseeds += hs->nseeds;
@@ -468,8 +502,7 @@ int Engine::finish_device(Staged &S) {
         }
       } else {
         if (int r = rec(ev_pool[2])) return r;
-        launch_match(ma, mblocks, stream);
-        ++stats.kernel_launches;
+        if (int r = launch_match_seq(ma, mblocks, bfs_levels)) return r;
         if (int r = rec(ev_pool[3])) return r;
         CK(cudaMemcpyAsync(h_sched.ptr, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
         if (S.nq_live)
@@ -718,7 +751,7 @@ int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
   const unsigned long long nseeds = hs->nseeds;
   struct Cand {
     int bps;
-    uint32_t split, dd, pack, merge;
+    uint32_t split, dd, pack, merge, bfs;
   };
   auto rearm = [&]() -> int {
     std::memset(hs, 0, sizeof(Sched));
@@ -750,8 +783,7 @@ int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
       t.pack_max = c.pack;
       t.merge_max = c.merge;
       CK(cudaEventRecord(e0, stream));
-      launch_match(t, num_sms * c.bps, stream);
-      ++stats.kernel_launches;
+      if (int r = launch_match_seq(t, num_sms * c.bps, c.bfs)) return r;
       CK(cudaEventRecord(e1, stream));
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
@@ -770,20 +802,28 @@ int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
     }
     return DSM_OK;
   };
-  const Cand cur{blocks / std::max(num_sms, 1), ma.split_min, ma.donate_depth, ma.pack_max, ma.merge_max};
+  const Cand cur{blocks / std::max(num_sms, 1), ma.split_min, ma.donate_depth, ma.pack_max, ma.merge_max,
+                 bfs_levels};
+  // stage 0: depth-first or breadth-first rows for the first 1 or 2 levels
+  std::vector<Cand> c0;
+  for (uint32_t bl : {0u, 1u, 2u}) c0.push_back({cur.bps, cur.split, cur.dd, cur.pack, cur.merge, bl});
+  float best0 = 1e30f, best1 = 1e30f, best2 = 1e30f;
+  Cand b0 = cur;
+  if (d_rows.ptr)
+    if (int rc = sweep(c0, true, b0, best0)) return rc;
   // stage 1: the intersection tile -- packed last level x merge threshold --
   // at the current launch shape
   std::vector<Cand> c1;
   for (uint32_t pk : {0u, 256u, 1024u, 4096u})
-    for (uint32_t mg : {0u, 64u, 256u}) c1.push_back({cur.bps, cur.split, cur.dd, pk, mg});
-  float best1 = 1e30f, best2 = 1e30f;
-  Cand b1 = cur, bc = cur;
-  if (int rc = sweep(c1, true, b1, best1)) return rc;
+    for (uint32_t mg : {0u, 64u, 256u}) c1.push_back({cur.bps, cur.split, cur.dd, pk, mg, b0.bfs});
+  Cand b1 = b0, bc = b0;
+  if (!stop)
+    if (int rc = sweep(c1, !d_rows.ptr, b1, best1)) return rc;
   // stage 2: blocks per SM x split threshold x donation depth, at that tile
   std::vector<Cand> c2;
   for (int bps = std::max(1, match_blocks_per_sm - 2); bps <= match_blocks_per_sm; ++bps)
     for (uint32_t split : {64u, 128u, 512u})
-      for (uint32_t dd : {1u, 2u}) c2.push_back({bps, split, dd, b1.pack, b1.merge});
+      for (uint32_t dd : {1u, 2u}) c2.push_back({bps, split, dd, b1.pack, b1.merge, b1.bfs});
   bc = b1;
   if (!stop)
     if (int rc = sweep(c2, false, bc, best2)) return rc;
@@ -793,6 +833,7 @@ int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
     donate_depth = bc.dd;
     pack_max = bc.pack;
     merge_max = bc.merge;
+    bfs_levels = bc.bfs;
     stats.tune_best_ms = best2;
   }
   ma.pack_max = pack_max;

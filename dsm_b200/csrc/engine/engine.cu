@@ -130,7 +130,7 @@ std::vector<DevBuf *> Engine::all_dev_bufs() {
                              &d_pair_off, &d_pair_ent, &d_upd, &d_bkey, &d_bidx, &d_binfo, &d_gflag,
                              &d_vtp, &d_dkey, &d_dhead, &d_dsel, &d_seeds, &d_sched, &d_jobs,
                              &d_job_seq, &d_out_seg, &d_out_tup, &d_segcnt, &d_misc, &d_hdr, &d_qlisted, &d_segwork,
-                             &d_rinfo, &d_rmark, &d_rlist, &d_rprev};
+                             &d_rinfo, &d_rmark, &d_rlist, &d_rprev, &d_rows};
   for (auto &q : slots) v.push_back(&q.bitmap);
   for (auto &q : slots) v.push_back(&q.filter_scratch);
   for (auto &q : slots) v.push_back(&q.filter_plan);

@@ -170,6 +170,9 @@ struct Engine {
   uint32_t split_min = 0, donate_depth = 0;  // donation granularity (0 = kernel default)
   uint32_t pack_max = 1024;                  // packed last level (entries per pass; 0: off)
   uint32_t merge_max = 64;                   // merge intersection up to this probe range (0: off)
+  uint32_t bfs_levels = 0;                   // breadth-first rows: levels beyond the seed (0: depth-first)
+  uint64_t bfs_rows = 1u << 20;              // row table capacity
+  DevBuf d_rows;
   bool tune_next = false;                    // autotune on the next batch
   int use_graph = 0;                         // replay the batch segments as CUDA graphs
   int stall_test = 0;                        // arm matcher launches with a task nobody finishes
@@ -253,6 +256,7 @@ struct Engine {
   bool capturing = false;
   int prepare_filter(uint32_t id);
   int launch_filter(uint32_t id, int mode, int force_full);
+  int launch_match_seq(const MatchArgs &ma, int blocks, uint32_t levels);
   RegionDevice region_dev();
   int region_init();
   int filter_state(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us, uint32_t *info);

@@ -134,12 +134,26 @@ struct MatchArgs {
   // walked in tiles against the whole chunk instead of searched per entry
   // (0: always searched)
   uint32_t merge_max;
+  // breadth-first rows: in a launch with bfs_stop > 0, a task that finds
+  // candidates completing bfs_stop positions (with at least two positions
+  // left) writes each prefix as a row to rows_out instead of descending,
+  // while the table has room (then it descends as usual); a launch with
+  // rows_in takes its tasks from those rows instead of the seeds
+  uint32_t bfs_stop;
+  JobRec *rows_out;
+  unsigned long long *rows_cnt;
+  unsigned long long rows_cap;
+  const JobRec *rows_in;
 };
 // Arms a matcher launch: outstanding = seeds (+ phantom, a task nothing
 // finishes: a test hook), every ring slot free for its first position.
 void launch_sched_init(Sched *sc, const BatchHdr *hdr, unsigned long long *job_seq, uint32_t job_ring,
                        cudaStream_t s, uint32_t phantom = 0);
 void launch_match(const MatchArgs &a, int blocks, cudaStream_t s);
+// Between the two launches of a breadth-first plan: the scheduler restarts
+// with the rows written so far as its tasks (counters of work done, the
+// result-table position and the error word carry over).
+void launch_rows_arm(Sched *sc, const unsigned long long *rows_cnt, unsigned long long rows_cap, cudaStream_t s);
 int match_max_blocks_per_sm();
 
 }  // namespace dsm

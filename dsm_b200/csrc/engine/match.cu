@@ -473,6 +473,45 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
     return true;
   };
 
+  // Breadth-first rows: the candidates m of level L (lane k: cw) become
+  // rows of L + 1 fixed positions.  One reservation per chunk, all or
+  // nothing (a bounded compare-and-swap loop); false: no room, nothing
+  // written.
+  auto write_rows = [&](uint32_t L, uint32_t m, uint32_t cw) -> bool {
+    const uint32_t cnt = __popc(m);
+    unsigned long long base = ~0ull;
+    if (lane == 0) {
+      unsigned long long cur = ld_volatile(*P.rows_cnt);
+      for (int tries = 0; tries < 64 && cur + cnt <= P.rows_cap; ++tries) {
+        const unsigned long long prev = atomicCAS(P.rows_cnt, cur, cur + cnt);
+        if (prev == cur) {
+          base = cur;
+          break;
+        }
+        cur = prev;
+      }
+    }
+    base = __shfl_sync(kFull, base, 0);
+    if (base == ~0ull) return false;
+    const uint32_t fsrc = __shfl_sync(kFull, my_f, (lane - 8) & 31);
+    uint32_t bits = m;
+    for (uint32_t r = 0; r < cnt; ++r) {
+      const uint32_t b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      const uint32_t cb = __shfl_sync(kFull, cw, b);
+      uint32_t word = 0;
+      if (lane == 0) word = upd;
+      else if (lane == 1) word = qo;
+      else if (lane == 2) word = L + 1;
+      else if (lane >= 8 && lane < 24) {
+        const uint32_t fi = lane - 8;
+        word = fi < L ? fsrc : (fi == L ? cb : 0u);
+      }
+      __stcg(reinterpret_cast<uint32_t *>(P.rows_out + base + r) + lane, word);
+    }
+    return true;
+  };
+
   uint32_t L = depth;
   setup_level(L, lo, hi);
   uint32_t dticks = 0;  // chunks since the last donation check
@@ -540,8 +579,10 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
 #pragma unroll
               for (uint32_t sh = 16; sh; sh >>= 1)
                 if (__shfl_sync(kFull, bv, k + sh - 1) < e) k += sh;
-              found = found || (__shfl_sync(kFull, bv, k) == e && t + k < nb);
-              if (__shfl_sync(kFull, bv, 31) >= emax) break;
+              const uint32_t at = __shfl_sync(kFull, bv, k);  // every lane shuffles
+              const uint32_t last = __shfl_sync(kFull, bv, 31);
+              if (at == e && t + k < nb) found = true;
+              if (last >= emax) break;
             }
             probes += ok ? 1u : 0u;
             ok = ok && found;
@@ -583,6 +624,8 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
         emit(m, w, L, 0xFFFFFFFFu, 0);
       } else if (kLM && pack_max && L + 2 == nq && m) {
         if (!pack_last(L, m, w, lw)) cur_mask = m;
+      } else if (P.bfs_stop == L + 1 && m) {
+        if (!write_rows(L, m, w)) cur_mask = m;
       } else {
         cur_mask = m;
       }
@@ -737,7 +780,7 @@ __device__ void run_task(const MatchArgs &P, const DevBatchEdges &bt, uint32_t n
 __global__ void k_sched_init(Sched *sc, const BatchHdr *hdr, unsigned long long *job_seq, uint32_t job_ring,
                              uint32_t phantom) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned long long seed_cap = hdr->seed_cap;
+  const unsigned long long seed_cap = hdr ? hdr->seed_cap : ~0ull;  // no header: tasks are rows
   for (uint32_t s = i; s < job_ring; s += gridDim.x * blockDim.x) job_seq[s] = s;
   if (i == 0) {
     unsigned long long n = sc->nseeds;
@@ -760,6 +803,9 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_match(MatchArgs P) {
   __shared__ PackStage s_stage[kLM ? 8 : 1];
   const uint32_t lane = threadIdx.x & 31;
   if (*P.abort_flag & kErrArena) return;  // the batch was refused before its insert
+  // an earlier launch of this batch failed (one read, the same for the warp:
+  // the word can change while the kernel runs)
+  if (__shfl_sync(kFull, lane == 0 ? ld_volatile(P.sc->error) : 0u, 0)) return;
   const uint32_t nupd = P.hdr->n;
   const DevBatchEdges bt{P.bt.bkey, P.bt.binfo, P.hdr->m};
   bool seeds_done = false;
@@ -771,7 +817,13 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_match(MatchArgs P) {
     if (kind == 0) break;
     slot = __shfl_sync(kFull, slot, 0);
     uint32_t upd, qo, depth, lo = 0, hi = 0, fval = 0;
-    if (kind == 1) {
+    if (kind == 1 && P.rows_in) {  // a row written by the previous launch
+      const uint32_t word = __ldcg(reinterpret_cast<const uint32_t *>(P.rows_in + slot) + lane);
+      upd = __shfl_sync(kFull, word, 0);
+      qo = __shfl_sync(kFull, word, 1);
+      depth = __shfl_sync(kFull, word, 2);
+      fval = __shfl_sync(kFull, word, (lane + 8) & 31);
+    } else if (kind == 1) {
       uint4 s = P.seeds[slot];
       upd = s.x;
       qo = s.y;
@@ -799,6 +851,19 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_match(MatchArgs P) {
 }
 
 }  // namespace
+
+__global__ void k_rows_arm(Sched *sc, const unsigned long long *rows_cnt, unsigned long long rows_cap) {
+  sc->seed_next.v = 0;
+  sc->push_cnt.v = 0;
+  sc->pop_cnt.v = 0;
+  sc->done.v = 0;
+  sc->outstanding.v = 0;
+  sc->nseeds = min(*rows_cnt, rows_cap);
+}
+
+void launch_rows_arm(Sched *sc, const unsigned long long *rows_cnt, unsigned long long rows_cap, cudaStream_t s) {
+  k_rows_arm<<<1, 1, 0, s>>>(sc, rows_cnt, rows_cap);
+}
 
 void launch_sched_init(Sched *sc, const BatchHdr *hdr, unsigned long long *job_seq, uint32_t job_ring,
                        cudaStream_t s, uint32_t phantom) {

@@ -76,10 +76,12 @@ const char *dsm_last_error(dsm_engine *e);
                                    this many levels below them (0 = default 2; 1..4) */
 #define DSM_OPT_AUTOTUNE 13     /* 1: the next batch times its matcher launch under each
                                    candidate setting on its own union graph -- first the
+                                   plan (DSM_OPT_BFS_LEVELS in {0, 1, 2}), then the
                                    intersection tile (DSM_OPT_PACK_MAX in {0, 256, 1024,
                                    4096} x DSM_OPT_MERGE_MAX in {0, 64, 256}), then resident
                                    blocks per SM x split threshold x donation depth -- and
-                                   keeps the fastest in DSM_OPT_PACK_MAX / DSM_OPT_MERGE_MAX /
+                                   keeps the fastest in DSM_OPT_BFS_LEVELS /
+                                   DSM_OPT_PACK_MAX / DSM_OPT_MERGE_MAX /
                                    DSM_OPT_WARPS_PER_SM / DSM_OPT_SPLIT_MIN /
                                    DSM_OPT_DONATE_DEPTH; its results
                                    are those of any setting.  Reads 1 until that batch ran. */
@@ -123,6 +125,16 @@ const char *dsm_last_error(dsm_engine *e);
                                    32-entry chunk by a ballot/shuffle merge over 32-entry tiles
                                    instead of a binary search per entry (default 64; 0: always
                                    searched; at most 2^16).  Results do not depend on it. */
+#define DSM_OPT_BFS_LEVELS 22    /* matcher plan: 0 (default) depth-first from the seeds; k in 1..8:
+                                   the first launch expands every seed breadth-first to
+                                   prefixes of 2 + k query vertices, written as rows (while
+                                   the row table has room, depth-first beyond it), and a
+                                   second launch matches depth-first from those rows -- the
+                                   reference's BFS join before its DFS matcher
+                                   (gpu_match.cu:1291-1357, join.cu:106-221).  Results do not
+                                   depend on it; DSM_OPT_AUTOTUNE tries 0, 1 and 2. */
+#define DSM_OPT_BFS_ROWS 23      /* row table capacity for DSM_OPT_BFS_LEVELS (default 2^20
+                                   rows of 128 bytes) */
 #define DSM_OPT_PACK_MAX 19     /* matcher intersection tile: the candidates one 32-entry
                                    chunk leaves at the second-to-last query vertex have
                                    their last-level ranges laid end to end and scanned

@@ -248,3 +248,43 @@ def test_intersection_tile_settings_agree(cfg, scale, nqs):
     # config 5's twelve-vertex cyclic queries match rarely: there the
     # bounded (flagged) searches are what the settings must agree on
     assert int(exact.astype(np.float64).sum()) > (1000 if cfg != 5 else 0) or (cfg == 5 and flagged > 0)
+
+
+@pytest.mark.parametrize("cfg,scale,nqs,form", [(2, -6, 3, "batched"), (3, -6, 32, "batched"), (3, -6, 8, "plain"),
+                                               (5, -4, 8, "graph")])
+def test_breadth_first_rows_agree(cfg, scale, nqs, form):
+    """DSM_OPT_BFS_LEVELS (breadth-first rows, then depth-first from them):
+    1 and 2 levels, and a row table of 64 rows (most prefixes go on
+    depth-first in place), give the listed results and work-limit flags of
+    the depth-first plan, and the first query's equal the oracle's."""
+    lim = 200_000
+    w = workload(cfg, scale_log2=scale, num_batches=1)
+    b = next(w.batches())[:512]
+    qs = w.queries[:nqs]
+    extra = {"plain": {"OPT_PLAIN": 1}, "graph": {"OPT_GRAPH": 1}}.get(form, {})
+    res = []
+    for lv, rows in ((0, 1 << 20), (1, 1 << 20), (2, 1 << 20), (2, 64)):
+        e, qids = _fresh(w.nv, w.labels, w.edges, qs, OPT_BFS_LEVELS=lv, OPT_BFS_ROWS=rows, OPT_WORK_LIMIT=lim,
+                         **extra)
+        if form == "graph":
+            e.run_batch(b[:5])  # captured on a small batch, replayed on the next
+            r = e.run_batch(b[5:])
+        else:
+            r = e.run_batch(b)
+        res.append(r)
+        e.close()
+    for r in res[1:]:
+        _same_flagged(res[0], r)
+    bb = b[5:] if form == "graph" else b
+    st = oracle_stream(w.nv, w.labels, w.edges, qs[0])
+    if form == "graph":
+        st.apply_graph(b[:5])
+    st.set_work_limit(lim)
+    s, c, t = st.apply(bb, listed=True)
+    r = res[1]
+    got = r.counts[r.query_index(qids[0])]
+    fo, fe = (c & d.INCOMPLETE) != 0, (got & d.INCOMPLETE) != 0
+    assert np.array_equal(fo, fe)
+    assert np.array_equal(got[~fe], c[~fo])
+    for i in range(len(bb)):
+        assert np.array_equal(r.tuples_of(qids[0], i), t[i] if not fo[i] else t[i][:0]), f"update {i}"
