@@ -104,7 +104,7 @@ int dsm_engine_set_option(dsm_engine *e, int option, int64_t value) {
       E.bfs_rows = (uint64_t)value;
       return DSM_OK;
     case DSM_OPT_MERGE_MAX:
-      if (value < 0 || value > (1 << 16)) return E.fail(DSM_ERR_ARG, "merge threshold 0..2^16 entries");
+      if (value < 0 || value > 4096) return E.fail(DSM_ERR_ARG, "merge threshold 0..4096 entries");
       E.merge_max = (uint32_t)value;
       return DSM_OK;
     case DSM_OPT_PACK_MAX:

@@ -370,7 +370,7 @@ int Engine::match_eager(Staged &S, MatchArgs &ma, SeedArgs &sa, int blocks) {
     if (int r = launch_match_seq(ma, blocks, bfs_levels)) return r;
     CK(cudaMemcpyAsync(hs, d_sched.ptr, sizeof(Sched), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
-    total.nseeds += hs->nseeds;
+    total.nseeds += hs->seeds ? hs->seeds : hs->nseeds;
     total.donations += hs->donations;
     total.steals += hs->steals;
     total.alg_bytes += hs->alg_bytes;
@@ -453,7 +453,7 @@ int Engine::finish_device(Staged &S) {
         break;
       }
       Sched *hs = (Sched *)h_sched.ptr;
-      const unsigned long long nseeds = S.sc.nseeds;
+      const unsigned long long nseeds = S.sc.seeds ? S.sc.seeds : S.sc.nseeds;  // rows plan: nseeds counts rows
       std::memset(hs, 0, sizeof(Sched));
       hs->nseeds = nseeds;
       CK(cudaMemcpyAsync(d_sched.ptr, hs, sizeof(Sched), cudaMemcpyHostToDevice, stream));
@@ -659,7 +659,7 @@ int Engine::assemble(Staged &S, BatchResult &R) {
     stats.updates += n;
     stats.matches += exact;
     stats.over_limit += incomplete;
-    stats.seeds += S.sc.nseeds;
+    stats.seeds += S.sc.seeds ? S.sc.seeds : S.sc.nseeds;
     stats.donations += S.sc.donations;
     stats.steals += S.sc.steals;
     stats.relocations += reloc;

@@ -136,7 +136,8 @@ struct Sched {
   unsigned long long alg_bytes;
   unsigned long long matches;  // embeddings counted (listed or not)
   unsigned int error;
-  unsigned int pad[5];
+  unsigned int pad;
+  unsigned long long seeds;    // seeds of the batch, kept when a second launch takes rows as tasks
 };
 
 // Bit 63 of a (query, update) count: the segment's search went over the

@@ -853,6 +853,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_match(MatchArgs P) {
 }  // namespace
 
 __global__ void k_rows_arm(Sched *sc, const unsigned long long *rows_cnt, unsigned long long rows_cap) {
+  sc->seeds = sc->nseeds;  // the seed table's count, for a rerun from the seeds
   sc->seed_next.v = 0;
   sc->push_cnt.v = 0;
   sc->pop_cnt.v = 0;

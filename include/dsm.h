@@ -124,7 +124,7 @@ const char *dsm_last_error(dsm_engine *e);
                                    of at most this many entries is intersected with a whole
                                    32-entry chunk by a ballot/shuffle merge over 32-entry tiles
                                    instead of a binary search per entry (default 64; 0: always
-                                   searched; at most 2^16).  Results do not depend on it. */
+                                   searched; at most 4096).  Results do not depend on it. */
 #define DSM_OPT_BFS_LEVELS 22    /* matcher plan: 0 (default) depth-first from the seeds; k in 1..8:
                                    the first launch expands every seed breadth-first to
                                    prefixes of 2 + k query vertices, written as rows (while

@@ -20,3 +20,13 @@ def _built():
         subprocess.run([sys.executable, os.path.join(ROOT, "dsm_b200", "build.py")], check=True)
     if not os.path.exists(os.path.join(ROOT, "oracle", "_build", "liboracle.so")):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+
+
+def pytest_runtest_logreport(report):
+    """With DSM_TEST_TIMES set to a path, each test's call time and outcome
+    are appended to that file as the test ends (readable even when the run is
+    cut short)."""
+    path = os.environ.get("DSM_TEST_TIMES")
+    if path and report.when == "call":
+        with open(path, "a") as f:
+            f.write(f"{report.duration:9.2f} {report.outcome:7s} {report.nodeid}\n")

@@ -226,7 +226,7 @@ def test_intersection_tile_settings_agree(cfg, scale, nqs):
     b = next(w.batches())[:1024]
     qs = w.queries[:nqs]
     res = []
-    for pk, mg in ((0, 0), (32, 256), (1024, 64), (1 << 20, 1 << 16)):
+    for pk, mg in ((0, 0), (32, 256), (1024, 64), (1 << 14, 1024)):
         e, qids = _fresh(w.nv, w.labels, w.edges, qs, OPT_PACK_MAX=pk, OPT_MERGE_MAX=mg, OPT_WORK_LIMIT=lim)
         assert e.get_option(d.OPT_PACK_MAX) == pk and e.get_option(d.OPT_MERGE_MAX) == mg
         res.append(e.run_batch(b))
