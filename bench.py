@@ -381,7 +381,7 @@ def run_serve(args, rank=0, world=1):
             assert again == ids, "the initial queries came back with other ids"
     clocks = sampler.stop()
     tuned = {k: e.get_option(getattr(d, "OPT_" + k.upper()))
-             for k in ("warps_per_sm", "split_min", "donate_depth", "pack_max", "merge_max")}
+             for k in ("warps_per_sm", "split_min", "donate_depth", "pack_max", "merge_max", "bfs_levels")}
 
     # the forms must agree request by request
     ref = runs["batched"]
@@ -575,7 +575,14 @@ def run_reference(args, rank):
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if not args.no_ref_host:
-        line["reference_update_host_graph"] = reference_update_host_graph(w, reqs[W:], 3, args.ref_host_s)
+        # updateHostGraph rebuilds the whole CSR through a std::set per vertex
+        # (about 20 GB of host memory at 2^28 edges): timed on the same stream
+        # at 1/16 scale
+        ws = orc.Workload(4, scale_log2=args.scale - 4, num_batches=8)
+        rh = reference_update_host_graph(ws, list(ws.batches()), 8, args.ref_host_s)
+        if rh is not None:
+            rh["sample"] += f"; config-4 stream at 1/16 scale (|V|=2^{20 + args.scale}, |E|=2^{24 + args.scale})"
+        line["reference_update_host_graph"] = rh
     return line
 
 
@@ -672,7 +679,7 @@ def run_step(args, rank, world):
                        "l2": "256 MiB buffer written between timed batches",
                        "filter": args.filter,
                        "tuned": {k: e.get_option(getattr(d, "OPT_" + k.upper()))
-                                 for k in ("warps_per_sm", "split_min", "donate_depth", "pack_max", "merge_max")}},
+                                 for k in ("warps_per_sm", "split_min", "donate_depth", "pack_max", "merge_max", "bfs_levels")}},
             "updates_per_sec": upd / (dev_ms / 1e3), "matches": matches,
             "latency_ms": {"p50": float(np.percentile(R[:, 1], 50)), "p99": float(np.percentile(R[:, 1], 99))},
             "e2e": {"value": matches / (wall_ms / 1e3), "unit": "matches/s",

@@ -247,7 +247,7 @@ int Engine::launch_front(Staged &S) {
   ma.out_seg = (uint32_t *)d_out_seg.ptr;
   ma.out_tup = (uint32_t *)d_out_tup.ptr;
   ma.cap = list_mode ? std::min<unsigned long long>(d_out_seg.bytes / 4, d_out_tup.bytes / 4 / ma.W) : 0;
-  int blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
+  int blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : default_blocks_per_sm());
 
   const bool tuning = tune_next && S.match && !S.plain;
   const bool graphed = use_graph && !tuning && !S.plain;
@@ -491,7 +491,7 @@ int Engine::finish_device(Staged &S) {
       ma.out_seg = (uint32_t *)d_out_seg.ptr;
       ma.out_tup = (uint32_t *)d_out_tup.ptr;
       ma.cap = std::min<unsigned long long>(d_out_seg.bytes / 4, d_out_tup.bytes / 4 / S.W);
-      const int mblocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
+      const int mblocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : default_blocks_per_sm());
       SeedArgs sa{g, dh, (const uint4 *)d_upd.ptr, (const uint32_t *)d_vtp.ptr, (const uint32_t *)d_pair_off.ptr,
                   (const uint32_t *)d_pair_ent.ptr, (const QDev *)d_qd.ptr, (const OrderRec *)d_orders.ptr,
                   (uint4 *)d_seeds.ptr, (Sched *)d_sched.ptr, kAllSlots};
@@ -840,7 +840,7 @@ int Engine::autotune(MatchArgs &ma, const Staged &S, int &blocks) {
   ma.merge_max = merge_max;
   ma.split_min = split_min;
   ma.donate_depth = donate_depth;
-  blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : match_blocks_per_sm);
+  blocks = num_sms * (warps_per_sm ? std::max(1, warps_per_sm / 8) : default_blocks_per_sm());
   return rearm();  // the batch's real launch starts from scratch
 }
 

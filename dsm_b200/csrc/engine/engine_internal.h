@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -145,7 +146,10 @@ struct Engine {
   cudaStream_t stream = nullptr;
   int num_sms = 148;
   int clock_khz = 1965000;
-  int match_blocks_per_sm = 2;
+  int match_blocks_per_sm = 2;  // most resident matcher blocks per SM (the tuner's upper end)
+  // untuned launch shape: 4 blocks per SM, the 64-register variant (the
+  // 48-register one spills; tuning on config 2 and 4 picked 4 and 3 blocks)
+  int default_blocks_per_sm() const { return std::max(1, std::min(match_blocks_per_sm, 4)); }
   std::mutex mu;
   std::mutex emu;          // guards last_error (written by the serving worker too)
   std::string last_error;
