@@ -74,6 +74,32 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+# Counters of the matcher measured by ncu (one B200, --clock-control none):
+# config 4 at 1/4 scale, launches 81-83 of `bench.py --scale -2 --steps 1
+# --warmup 1`; config 2 at full size, the timed launch of `bench.py --mode
+# step --steps 1 --warmup 1 --autotune 0` (5 blocks per SM).
+C4_NCU = {"dram_bytes_per_launch": 1.672e8, "l2_bytes_per_launch": 2.385e9, "launch_ms": 1.825,
+          "l2_hit": 0.620, "issue_active": 0.180}
+C2_NCU = {"dram_bytes_per_launch": 4.847e8, "l2_bytes_per_launch": None, "launch_ms": 225.4,
+          "l2_hit": 0.939, "issue_active": 0.395}
+
+
+def l2_figures(ncu):
+    """L2 side of the roofline: the ncu L2 bytes per launch over the ncu
+    launch time against an L2 copy bandwidth measured here."""
+    out = {"hit_rate": ncu["l2_hit"]}
+    try:
+        peak = measure_l2_gbs()
+    except Exception as ex:  # the figure is context; the line stands without it
+        peak, out["peak_error"] = None, str(ex)
+    out["peak_gbs"] = peak
+    if ncu.get("l2_bytes_per_launch"):
+        gbs = ncu["l2_bytes_per_launch"] / (ncu["launch_ms"] / 1e3) / 1e9
+        out["ncu_gbs"] = gbs
+        out["frac"] = gbs / peak if peak else None
+    return out
+
+
 def measure_l2_gbs():
     """L2 copy bandwidth (read + write bytes per second) measured here: a
     16 MiB -> 16 MiB copy repeated, both buffers resident in the 126 MB L2,
@@ -454,8 +480,16 @@ def run_serve(args, rank=0, world=1):
             "p99_ratio": (forms["plain"]["poisson"]["p99_ms"] or 0) / max(sv["poisson"]["p99_ms"] or 1e-9, 1e-9)},
         "gpu_launches": sv["kernel_launches_burst"],
         "roofline": {"bound": "hbm", "kernel": "k_match", "achieved": alg / 1e9 / (match_ms / 1e3) if match_ms else 0,
-                     "peak": peak, "unit": "GB/s", "peak_source": peak_kind, "traffic": None,
-                     "note": "algorithmic bytes of the matcher over the served device time of the burst"},
+                     "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
+                     # ncu, this workload at 1/4 scale (same request sizes): DRAM
+                     # read + write, L2 bytes and issue activity per k_match launch
+                     "traffic": C4_NCU["dram_bytes_per_launch"],
+                     "traffic_note": "ncu dram__bytes read+write per k_match launch, mean of 3 launches of this "
+                                     "workload at 1/4 scale (same request sizes)",
+                     "l2": l2_figures(C4_NCU),
+                     "issue_active": C4_NCU["issue_active"],
+                     "note": "algorithmic bytes of the matcher over the served device time of the burst; the "
+                             "matcher waits on dependent L2 loads (issue_active), HBM is not the binding bound"},
         "clocks": clocks,
         "gen_seconds": gen_s,
         "load_seconds": load_s,
@@ -687,7 +721,11 @@ def run_step(args, rank, world):
                     "d2h_bytes_per_step": int(len(queries) * len(batches[-1]) * 8 + len(batches[-1]))},
             "gpu_launches": int(R[:, 5].sum()), "donations": int(R[:, 6].sum()), "steals": int(R[:, 7].sum()),
             "roofline": {"bound": "hbm", "kernel": "k_match", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None},
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": C2_NCU["dram_bytes_per_launch"] if args.config == 2 and args.scale == 0 else None,
+                         "traffic_note": "ncu dram__bytes read+write of one k_match launch on this workload",
+                         "l2": l2_figures(C2_NCU) if args.config == 2 and args.scale == 0 else None,
+                         "issue_active": C2_NCU["issue_active"] if args.config == 2 and args.scale == 0 else None},
             "clocks": clocks, "gen_seconds": gen_s}
     e.close()
     return line
