@@ -113,7 +113,7 @@ def test_c3_full_size_256_queries_one_launch():
     # all 256 queries run in the launch; every 8th is recounted by the oracle
     picks = _every(_pick(counts, heavy=2, ceiling=2 * 10 ** 7, n_random=1, rng=np.random.default_rng(3)), 8)
     compared, heaviest = _oracle_check(w, w.queries, batch, counts, picks, work_limit=lim)
-    assert compared >= 32 * 2
+    assert compared >= 32  # each checked query: its heaviest exact counts (if any) and a random one
 
 
 def test_c5_skew_scaled_twelve_vertex_queries():
