@@ -102,9 +102,21 @@ __global__ void k_ldf_nlf(DevGraph g, QFilterDesc *D, uint32_t *vcand, uint32_t 
     if (keep) {
       cnt[wib][lane] = 0;
       __syncwarp();
+      // the run starts on a 16-byte boundary: four entries per lane per load
       const uint32_t *run = adj_list(g, av);
-      for (uint32_t k = lane; k < av.y; k += 32) {
-        uint32_t l = g.lab[run[k] & kIdMask] & kLabelMask;
+      const uint4 *run4 = reinterpret_cast<const uint4 *>(run);
+      const uint32_t n4 = av.y >> 2;
+      for (uint32_t k = lane; k < n4; k += 32) {
+        const uint4 q = run4[k];
+        const uint32_t e[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const uint32_t l = g.lab[e[t] & kIdMask] & kLabelMask;
+          if (l < nl) atomicAdd(&cnt[wib][l], 1u);
+        }
+      }
+      for (uint32_t k = 4 * n4 + lane; k < av.y; k += 32) {
+        const uint32_t l = g.lab[run[k] & kIdMask] & kLabelMask;
         if (l < nl) atomicAdd(&cnt[wib][l], 1u);
       }
       __syncwarp();
@@ -323,7 +335,16 @@ __global__ void k_region_expand(DevGraph g, RegionDevice rg, uint32_t hop) {
     const uint32_t v = rg.list[i];
     const uint2 av = g.adj[v];
     const uint32_t *run = adj_list(g, av);
-    for (uint32_t k = lane; k < av.y; k += 32) claim(rg, epoch, run[k] & kIdMask, hop);
+    const uint4 *run4 = reinterpret_cast<const uint4 *>(run);  // 16-byte aligned run
+    const uint32_t n4 = av.y >> 2;
+    for (uint32_t k = lane; k < n4; k += 32) {
+      const uint4 q = run4[k];
+      claim(rg, epoch, q.x & kIdMask, hop);
+      claim(rg, epoch, q.y & kIdMask, hop);
+      claim(rg, epoch, q.z & kIdMask, hop);
+      claim(rg, epoch, q.w & kIdMask, hop);
+    }
+    for (uint32_t k = 4 * n4 + lane; k < av.y; k += 32) claim(rg, epoch, run[k] & kIdMask, hop);
     if (*(volatile const uint32_t *)&rg.info->ov_round < 64) return;
   }
 }
