@@ -22,12 +22,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "../../../include/dsm.h"
+#include "../host/par.h"
 #include "engine_internal.h"
 #include "filter.cuh"
 #include "kernels.cuh"
@@ -625,15 +628,34 @@ int Engine::assemble(Staged &S, BatchResult &R) {
   R.tuples.clear();
   if (S.listed) {
     R.tuples.resize(R.offsets.back());
-    std::vector<uint64_t> cur(R.offsets.begin(), R.offsets.end() - 1);
     const uint32_t *hs = (const uint32_t *)H.out_seg.ptr, *ht = (const uint32_t *)H.out_tup.ptr;
-    for (size_t r = 0; r < S.cnt; ++r) {
-      const uint32_t s = hs[r];
-      const uint32_t ql = s / n;
-      if (!R.qlisted[ql] || (R.counts[s] & kCountIncomplete)) continue;  // partial tuples
-      const uint32_t w = R.widths[ql];
-      std::memcpy(&R.tuples[cur[s]], ht + r * S.W, w * 4);
-      cur[s] += w;
+    const size_t nseg = (size_t)nql * n;
+    if (S.cnt < (1u << 16)) {
+      std::vector<uint64_t> cur(R.offsets.begin(), R.offsets.end() - 1);
+      for (size_t r = 0; r < S.cnt; ++r) {
+        const uint32_t s = hs[r];
+        const uint32_t ql = s / n;
+        if (!R.qlisted[ql] || (R.counts[s] & kCountIncomplete)) continue;  // partial tuples
+        const uint32_t w = R.widths[ql];
+        std::memcpy(&R.tuples[cur[s]], ht + r * S.W, w * 4);
+        cur[s] += w;
+      }
+    } else {
+      // on all host threads: each tuple claims its place in its segment by an
+      // atomic cursor (the order inside a segment is the device's, which is
+      // unordered anyway; the sort below makes it canonical)
+      std::unique_ptr<std::atomic<uint64_t>[]> cur(new std::atomic<uint64_t>[nseg]);
+      for (size_t k = 0; k < nseg; ++k) cur[k].store(R.offsets[k], std::memory_order_relaxed);
+      parallel_for(S.cnt, 1u << 15, [&](size_t lo, size_t hi) {
+        for (size_t r = lo; r < hi; ++r) {
+          const uint32_t s = hs[r];
+          const uint32_t ql = s / n;
+          if (!R.qlisted[ql] || (R.counts[s] & kCountIncomplete)) continue;  // partial tuples
+          const uint32_t w = R.widths[ql];
+          const uint64_t p = cur[s].fetch_add(w, std::memory_order_relaxed);
+          std::memcpy(&R.tuples[p], ht + r * S.W, w * 4);
+        }
+      });
     }
     if (S.sort) {
       std::vector<uint64_t> cnt_listed(R.counts);
