@@ -13,6 +13,8 @@ update without applying it).  Counts must be equal.
 - config 3: 256 queries of 4-12 vertices on the full-size graph, one
   512-update slice, all queries in one launch (every 8th query recounted;
   each search bounded by a work limit of 2^22, flags checked alike);
+- config 4 at full size (2^24 vertices, 2^28 edges): the benchmark's first
+  request against all 64 queries under its work limit;
 - config 5 at 1/16 scale (2^18 vertices, 2^23 edges, hubs above 10^4): 64
   twelve-vertex cyclic queries, one 65,536-update batch, 80 % deletions
   (every 4th query recounted).
@@ -128,3 +130,20 @@ def test_c5_skew_scaled_twelve_vertex_queries():
     compared, heaviest = _oracle_check(w, w.queries, batch, counts, picks, work_limit=lim)
     assert compared >= 16
     assert st["donations"] > 0
+
+
+def test_c4_full_size_first_request_64_queries():
+    """The benchmark's own workload at full size (R-MAT 2^24 vertices, 2^28
+    edges, 32 labels): its first request (211 updates) against all 64
+    queries of 4-10 vertices in one launch, each search bounded by the
+    benchmark's work limit (2^18).  For every query the oracle recounts its
+    two heaviest exact updates and a random one (flags compared alike)."""
+    lim = 1 << 18
+    w = workload(4, num_batches=1)
+    batch = next(w.batches())
+    counts, signs, st = _engine_counts(w, w.queries, batch, work_limit=lim)
+    assert counts.shape[0] == 64
+    picks = _pick(counts, heavy=2, ceiling=10 ** 9, n_random=1, rng=np.random.default_rng(4))
+    compared, heaviest = _oracle_check(w, w.queries, batch, counts, picks, work_limit=lim)
+    assert compared >= 64
+    assert heaviest > 0
