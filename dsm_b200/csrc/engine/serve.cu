@@ -15,6 +15,7 @@
 #include <chrono>
 #include <cstring>
 
+#include "../host/par.h"
 #include "engine_internal.h"
 
 namespace dsm {
@@ -263,8 +264,17 @@ void Engine::post_batch(InFlight &b) {
   }
   const uint32_t N = (uint32_t)b.all.size();
   const uint32_t nql = (uint32_t)R.qids.size();
-  std::vector<std::unique_ptr<BatchResult>> outs;
-  for (size_t k = 0; k < b.reqs.size(); ++k) {
+  std::vector<std::unique_ptr<BatchResult>> outs(b.reqs.size());
+  if (b.reqs.size() == 1) {  // one request: its result is the batch's, moved
+    auto o = std::make_unique<BatchResult>(std::move(R));
+    o->id = b.reqs[0].id;
+    o->merged_requests = 1;
+    o->merged_updates = N;
+    outs[0] = std::move(o);
+  }
+  // merged requests: each request's slice of every per-(query, update) array,
+  // the requests on host threads
+  parallel_chunks(b.reqs.size() == 1 ? 0 : b.reqs.size(), [&](size_t k) {
     const uint32_t s = b.start[k], n = b.start[k + 1] - s;
     auto o = std::make_unique<BatchResult>();
     o->id = b.reqs[k].id;
@@ -293,8 +303,8 @@ void Engine::post_batch(InFlight &b) {
     o->match_ms = R.match_ms;
     o->merged_requests = (uint32_t)b.reqs.size();
     o->merged_updates = N;
-    outs.push_back(std::move(o));
-  }
+    outs[k] = std::move(o);
+  });
   const auto t1 = std::chrono::steady_clock::now();
   {
     std::lock_guard<std::mutex> r(rmu);
