@@ -665,8 +665,12 @@ def run_step(args, rank, world):
     for q in queries:
         e.register(q)
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MiB > L2
-    for b in batches[:args.warmup]:
+    print(f"[bench] config {args.config}: {w.nv} vertices, {len(w.edges)} edges, {len(queries)} queries, "
+          f"batches of {len(batches[0])}, generated in {gen_s:.0f} s", file=sys.stderr, flush=True)
+    for k, b in enumerate(batches[:args.warmup]):
+        t = time.perf_counter()
         e.run_batch(b)
+        print(f"[bench] warm-up batch {k}: {time.perf_counter() - t:.2f} s", file=sys.stderr, flush=True)
     sampler = ClockSampler(dev)
     if rank == 0:
         sampler.start()
