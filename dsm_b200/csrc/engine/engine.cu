@@ -759,12 +759,17 @@ int Engine::launch_filters() {
   uint32_t hops = 0;
   for (uint32_t id : live_ids) hops = std::max(hops, std::min<uint32_t>(slots[id].filter_hops, kRegionMaxHops));
   const uint32_t *hdr_n = (const uint32_t *)d_hdr.ptr;  // BatchHdr::n
-  launch_region_build(dev_graph(), region_dev(), hdr_n, (const uint4 *)d_upd.ptr, hops, num_sms, stream);
-  stats.kernel_launches += 3 + 2 * hops;
+  const bool region = d_rinfo.ptr != nullptr;  // without its buffers every run is full
+  if (region) {
+    launch_region_build(dev_graph(), region_dev(), hdr_n, (const uint4 *)d_upd.ptr, hops, num_sms, stream);
+    stats.kernel_launches += 3 + 2 * hops;
+  }
   for (uint32_t id : live_ids)
     if (int rc = launch_filter(id, filter_mode, 0)) return rc;
-  launch_region_save(region_dev(), hdr_n, (const uint4 *)d_upd.ptr, stream);
-  ++stats.kernel_launches;
+  if (region) {
+    launch_region_save(region_dev(), hdr_n, (const uint4 *)d_upd.ptr, stream);
+    ++stats.kernel_launches;
+  }
   if (int r = rec(f1)) return r;
   filter_timed = true;
   return DSM_OK;
@@ -818,8 +823,9 @@ int Engine::filter_state(uint32_t qid, uint32_t *bitmaps, uint32_t *v_cand_us, u
   if (v_cand_us) CK(cudaMemcpyAsync(v_cand_us, s.filter_scratch.ptr, (size_t)nv * 4, cudaMemcpyDeviceToHost, stream));
   QFilterDesc desc;
   RegionInfo I;
+  std::memset(&I, 0, sizeof(I));
   CK(cudaMemcpyAsync(&desc, s.filter_plan.ptr, sizeof(desc), cudaMemcpyDeviceToHost, stream));
-  CK(cudaMemcpyAsync(&I, d_rinfo.ptr, sizeof(I), cudaMemcpyDeviceToHost, stream));
+  if (d_rinfo.ptr) CK(cudaMemcpyAsync(&I, d_rinfo.ptr, sizeof(I), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
   if (info) {
     info[0] = desc.full_now;
