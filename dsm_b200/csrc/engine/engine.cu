@@ -276,6 +276,7 @@ int Engine::region_init() {
   CK(cudaMemsetAsync(d_rmark.ptr, 0, (size_t)std::max<uint32_t>(nv, 1) * 4, stream));
   CK(cudaMemcpyAsync(d_rinfo.ptr, &I, sizeof(I), cudaMemcpyHostToDevice, stream));
   CK(cudaStreamSynchronize(stream));  // `I` is stack memory
+  region_batches = 0;
   return DSM_OK;
 }
 
@@ -732,6 +733,12 @@ int Engine::launch_filter(uint32_t id, int mode, int force_full) {
 // (host: buffers, plans, descriptors) runs before the batch's device work;
 // launch_filters only enqueues kernels and events.
 int Engine::prepare_filters() {
+  // the region's vertex marks carry a 26-bit epoch, one per filtered batch:
+  // start afresh before it wraps (every query's next run is then full)
+  if (filter_mode > 0 && ++region_batches >= (1u << 26) - 4) {
+    if (int rc = region_init()) return rc;
+    region_batches = 0;
+  }
   bool changed = false;
   for (uint32_t id : live_ids) {
     QDev &q = qd_host[id];

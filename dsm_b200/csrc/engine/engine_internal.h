@@ -201,6 +201,7 @@ struct Engine {
   DevBuf d_lab, d_adj, d_cap, d_arena, d_arena_top, d_loff;
   // incremental filter region (filter.cuh RegionInfo)
   DevBuf d_rinfo, d_rmark, d_rlist, d_rprev;
+  uint64_t region_batches = 0;  // filtered batches since the region buffers were set up
   int filter_incremental = 1;
 
   // queries
