@@ -9,7 +9,12 @@
 // run of the backward neighbour with the fewest neighbours (the pivot): each
 // lane tests one element (label, injectivity, filter bit, membership in the
 // other backward neighbours' runs, liveness at the update's view time) and a
-// ballot gives the chunk's candidate mask.  Nothing is materialised.
+// ballot gives the chunk's candidate mask.  Membership in a short range is
+// a warp merge over 32-entry tiles, in a long one a binary search; the last
+// level of a chunk's candidates is evaluated in one packed pass, with the
+// longest shared range staged in shared memory.  Nothing is materialised,
+// except, with breadth-first levels, the rows a first launch hands to a
+// second.
 //
 // Scheduling.  Tasks are first the seeds (one atomicAdd each), then donated
 // jobs.  An idle warp takes a ticket (one atomicAdd on pop_cnt) and waits for
