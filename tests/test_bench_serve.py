@@ -131,3 +131,22 @@ def test_cpu_sample_tiny():
 def test_summarize():
     s = bench.summarize([1.0, 2.0, 3.0, 100.0], 50, 10, 2.0)
     assert s["p50_ms"] == 2.5 and s["matches_per_sec"] == 25.0 and s["updates_per_sec"] == 5.0
+
+
+def test_step_workload_names_and_l2_figures_without_gpu():
+    """The step mode names each configuration by what it is; the L2 side of
+    the roofline degrades to no peak (and no fraction) where the copy probe
+    cannot run, instead of failing the line."""
+    args = SimpleNamespace(config=2, scale=0)
+    assert "config2" in bench.step_workload(args, 3, 4096) and "4096" in bench.step_workload(args, 3, 4096)
+    args = SimpleNamespace(config=5, scale=-4)
+    name = bench.step_workload(args, 64, 65536)
+    assert "config5" in name and "2^18" in name and "twelve-vertex" in name
+    import torch
+    if torch.cuda.is_available():
+        return
+    out = bench.l2_figures(bench.C4_NCU)
+    assert out["peak_gbs"] is None and out["frac"] is None
+    assert out["ncu_gbs"] > 0 and 0 < out["hit_rate"] < 1
+    out2 = bench.l2_figures(bench.C2_NCU)  # no L2 byte count: hit rate only
+    assert "ncu_gbs" not in out2
